@@ -1,0 +1,34 @@
+"""polar_b200 — B200-native (sm_100a) solve-and-score path of POLAR.
+
+Drop-in for the entry points of realworld/polar_gpu.py that the drivers call
+(`import polar_b200 as pg`): Graph, Op, msolve, composite, poles, sketches, polar,
+true_marginals, degree_greedy, random_set, chunk_width.  The compute runs in the
+hand-written kernels of libpolar.so (include/polar.h) through ctypes; there is no CPU
+fallback.  Keyword-only extensions: precision='fp64'|'mixed', K=<fixed pole count>.
+"""
+from .quadrature import composite, fixed_rule, poles
+from .sketch import sketches, chunk_width
+from .synth import chung_lu, candidates
+
+__version__ = "0.1.0"
+
+_DEVICE_NAMES = ("Graph", "Op", "msolve", "Counter", "polar", "true_marginals", "degree_greedy", "random_set")
+
+
+def __getattr__(name):
+    # Device-side names load libpolar.so on first use, so host-only helpers (quadrature,
+    # sketches, generators) import on machines without a GPU.
+    if name in ("Graph", "Op"):
+        from . import graph
+        return getattr(graph, name)
+    if name in ("msolve", "Counter"):
+        from . import solver
+        return getattr(solver, name)
+    if name in ("polar", "true_marginals", "degree_greedy", "random_set"):
+        from . import greedy
+        return getattr(greedy, name)
+    raise AttributeError(name)
+
+
+__all__ = ["composite", "fixed_rule", "poles", "sketches", "chunk_width", "chung_lu", "candidates",
+           *_DEVICE_NAMES]

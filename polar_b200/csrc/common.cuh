@@ -1,0 +1,158 @@
+// Shared device helpers for libpolar (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "polar.h"
+
+#define POLAR_HD __host__ __device__ __forceinline__
+#define POLAR_D __device__ __forceinline__
+
+namespace polar {
+
+// ---------------------------------------------------------------------------------------
+// Vector access: V consecutive elements of T through one 4/8/16-byte load or store.
+template <typename T, int V> struct VecType;
+template <> struct VecType<float, 1> { using type = float; };
+template <> struct VecType<float, 2> { using type = float2; };
+template <> struct VecType<float, 4> { using type = float4; };
+template <> struct VecType<double, 1> { using type = double; };
+template <> struct VecType<double, 2> { using type = double2; };
+
+template <typename T, int V>
+union VecU {
+  typename VecType<T, V>::type v;
+  T a[V];
+};
+
+template <typename T, int V>
+POLAR_D void vload(T (&out)[V], const T* p) {
+  VecU<T, V> u;
+  u.v = *reinterpret_cast<const typename VecType<T, V>::type*>(p);
+#pragma unroll
+  for (int i = 0; i < V; ++i) out[i] = u.a[i];
+}
+
+// L2-only load for data that other CTAs of the same persistent launch rewrite.
+template <typename T, int V>
+POLAR_D void vload_cg(T (&out)[V], const T* p) {
+  VecU<T, V> u;
+  u.v = __ldcg(reinterpret_cast<const typename VecType<T, V>::type*>(p));
+#pragma unroll
+  for (int i = 0; i < V; ++i) out[i] = u.a[i];
+}
+
+template <typename T, int V>
+POLAR_D void vstore(T* p, const T (&in)[V]) {
+  VecU<T, V> u;
+#pragma unroll
+  for (int i = 0; i < V; ++i) u.a[i] = in[i];
+  *reinterpret_cast<typename VecType<T, V>::type*>(p) = u.v;
+}
+
+// ---------------------------------------------------------------------------------------
+POLAR_D uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+POLAR_D unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+POLAR_D void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+POLAR_D int ld_volatile_i32(const int* p) { return *reinterpret_cast<const volatile int*>(p); }
+
+// ---------------------------------------------------------------------------------------
+// Grid barrier for a cooperative (co-resident) launch.  Arrival: every CTA fences its
+// writes and bumps `count`; the last CTA to arrive may run serial work (a reduction of
+// per-CTA partials) before it releases the others by advancing `gen`.  Waiting CTAs
+// poll `gen` with a time limit; on expiry they record POLAR_ERR_TIMEOUT in `err` and
+// every CTA leaves the kernel at its next barrier.  No wait is unbounded.
+struct GridSync {
+  unsigned* count;
+  unsigned* gen;
+  int* err;
+  int* where;
+  uint64_t timeout_ns;
+};
+
+// Returns true in every thread of the last-arriving CTA.  `my_gen` receives the
+// generation to wait on.  Caller must later call grid_release (last CTA) or
+// grid_wait (others).
+POLAR_D bool grid_arrive(const GridSync& s, unsigned& my_gen) {
+  __shared__ unsigned sh_last, sh_gen;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned g = ld_acquire_u32(s.gen);
+    __threadfence();
+    unsigned old = atomicAdd(s.count, 1u);
+    sh_last = (old == gridDim.x - 1) ? 1u : 0u;
+    sh_gen = g;
+    if (sh_last) __threadfence();
+  }
+  __syncthreads();
+  my_gen = sh_gen;
+  return sh_last != 0;
+}
+
+// Releases the waiting CTAs.  Returns true (uniformly across the CTA) when no error has
+// been recorded.
+POLAR_D bool grid_release(const GridSync& s, unsigned my_gen) {
+  __shared__ int sh_ok2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *s.count = 0u;
+    __threadfence();
+    st_release_u32(s.gen, my_gen + 1u);
+    sh_ok2 = ld_volatile_i32(s.err) == 0;
+  }
+  __syncthreads();
+  return sh_ok2 != 0;
+}
+
+// Returns false (in all threads of the CTA) when the kernel must stop: a wait timed out
+// here or an error was recorded elsewhere.
+POLAR_D bool grid_wait(const GridSync& s, unsigned my_gen, int where) {
+  __shared__ int sh_ok;
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    uint64_t t0 = globaltimer_ns();
+    while (ld_acquire_u32(s.gen) == my_gen) {
+      if (ld_volatile_i32(s.err) != 0) { ok = 0; break; }
+      if (globaltimer_ns() - t0 > s.timeout_ns) {
+        atomicCAS(s.err, 0, (int)POLAR_ERR_TIMEOUT);
+        atomicCAS(s.where, 0, where);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    if (ld_volatile_i32(s.err) != 0) ok = 0;
+    sh_ok = ok;
+  }
+  __syncthreads();
+  return sh_ok != 0;
+}
+
+// Plain barrier (no serial section).
+POLAR_D bool grid_sync(const GridSync& s, int where) {
+  unsigned g;
+  if (grid_arrive(s, g)) return grid_release(s, g);
+  return grid_wait(s, g, where);
+}
+
+POLAR_HD int next_pow2(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace polar

@@ -1,0 +1,770 @@
+// Persistent multi-shift CG for POLAR (sm_100a).
+//
+// Replaces realworld/polar_gpu.py:88-133 (msolve).  One cooperative launch runs every
+// iteration of the seed CG for all R columns, the zeta recurrences of all p poles and the
+// three-scalar norm tracker, with bounded grid barriers between the phases:
+//
+//   P1  v = (M + tau_0 I) d  (CSR SpMM, heavy rows split)  + per-CTA partials of d.v
+//   R1  last CTA: a = rr / d.v
+//   P2  r <- r - a v ; partials of r.r ; r on the active rows -> history slot
+//   R2  last CTA: beta, zeta recurrences, tracker, freezing, convergence; the
+//       per-pole step coefficients (a_j, zeta_j, beta_j) of this iteration -> table
+//   P3  d <- r + beta d
+//   P4  every M iterations (and at exit): the deferred shifted update.  For each
+//       active row / column / pole, M steps of  X += a_j P ; P = zeta_j r + beta_j P
+//       are applied from the history in registers: X and P cross HBM once per M
+//       iterations instead of once per iteration.  The arithmetic per element is the
+//       same sequence of operations as the per-iteration update.
+//
+// Poles whose iterates are frozen for a whole block of M steps are skipped.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "graph_ops.cuh"
+#include "host_util.h"
+
+namespace polar {
+
+constexpr int kBlock = 512;
+constexpr int kWarps = kBlock / 32;
+constexpr int kMaxLd = 128;
+constexpr int kHist = 16;  // M: iterations per deferred shifted-update pass
+
+template <typename T> struct SolvePrm {
+  polar_graph g;
+  int n, R, ld, p, nA;
+  double tol;
+  long long maxit;
+  int track;
+  const double* W;
+  int ldw;
+  const double* tau;
+  const int* active;
+  const int* active_pos;
+  void* Xout;
+  int x_f32, ldx;
+  double* h_out;
+  long long* iters_out;
+  // workspace
+  T *r, *d, *v, *hist, *Pb, *Xb;
+  typename AccOf<T>::type* chunk_part;
+  int* hcount;
+  double* part;
+  double *rr, *stop, *ap, *bp, *ag, *beg, *chig;
+  int *act, *upd;
+  double *z, *zp, *hs, *ip, *pn;
+  int *live, *pflag;
+  T *ca, *cz, *cb;
+  int* ctl;  // [0]=status [1]=err [2]=where [3]=any  [4..5]=barrier count/gen
+  long long* stats;  // [0]=iterations [1]=flushes
+  uint64_t timeout_ns;
+};
+
+// ---------------------------------------------------------------------------------------
+template <int VEC>
+POLAR_D void reduce_cols_to_part(double (&acc)[VEC], int G, int ld, double* red, double* out_row) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = G; o < 32; o <<= 1)
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+  if (lane < G)
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) red[warp * ld + lane * VEC + v] = acc[v];
+  __syncthreads();
+  for (int c = threadIdx.x; c < ld; c += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < kWarps; ++w) s += red[w * ld + c];
+    out_row[c] = s;
+  }
+}
+
+// Sum of per-CTA partials part[b][c] over b in a fixed order (deterministic).
+POLAR_D void reduce_partials(const double* part, int nblk, int ld, double* tmp, double* out) {
+  const int S = blockDim.x / ld;
+  const int t = threadIdx.x, c = t % ld, s = t / ld;
+  if (s < S) {
+    double acc = 0.0;
+    for (int b = s; b < nblk; b += S) acc += __ldcg(part + (size_t)b * ld + c);
+    tmp[s * ld + c] = acc;
+  }
+  __syncthreads();
+  if (t < ld) {
+    double acc = 0.0;
+    for (int s2 = 0; s2 < S; ++s2) acc += tmp[s2 * ld + t];
+    out[t] = acc;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------
+template <typename T, int VEC, bool WEIGHTED>
+POLAR_D void spmm_phase(const polar_graph& g, const RowGroup& rg, int gid, int GT, double shift, const T* X,
+                        T* Y, int ld, typename AccOf<T>::type* chunk_part, int* hcount, double (&dacc)[VEC]) {
+  using A = typename AccOf<T>::type;
+  for (int ch = gid; ch < g.nchunks; ch += GT) {
+    const int h = __ldg(g.d_chunk_row + ch);
+    const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
+    A acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc);
+    vstore<A, VEC>(chunk_part + (size_t)ch * ld + rg.col, acc);
+    __threadfence();
+    __syncwarp(rg.mask);
+    int old = 0;
+    if (rg.lg == 0) old = atomicAdd(hcount + h, 1);
+    old = __shfl_sync(rg.mask, old, 0, rg.G);
+    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
+    if (old == c1 - c0 - 1) {
+      __threadfence();
+      A sum[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) sum[v] = A(0);
+      for (int c2 = c0; c2 < c1; ++c2) {
+        A pv[VEC];
+        vload_cg<A, VEC>(pv, chunk_part + (size_t)c2 * ld + rg.col);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
+      }
+      const int i = __ldg(g.d_hrow + h);
+      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+      T xi[VEC], yi[VEC];
+      finish_row<T, VEC>(g, rg, i, deg, shift, X, ld, sum, Y, ld, xi, yi);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+      if (rg.lg == 0) hcount[h] = 0;
+    }
+  }
+  for (int i = gid; i < g.n; i += GT) {
+    const int lo = __ldg(g.d_indptr + i), hi = __ldg(g.d_indptr + i + 1);
+    if (hi - lo > g.heavy_thresh) continue;
+    A acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc);
+    T xi[VEC], yi[VEC];
+    finish_row<T, VEC>(g, rg, i, hi - lo, shift, X, ld, acc, Y, ld, xi, yi);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Deferred shifted update over `nsteps` recorded iterations.  Thread item = (tile of E
+// active rows, column c); the E rows share the per-(pole, step, column) coefficients.
+template <typename T, int E>
+POLAR_D void shifted_update(const SolvePrm<T>& P, int nsteps, bool first, bool final_pass, long long tid,
+                            long long nth) {
+  const int ld = P.ld, nA = P.nA, p = P.p;
+  const int ntile = (nA + E - 1) / E;
+  const long long items = (long long)ntile * ld;
+  for (long long item = tid; item < items; item += nth) {
+    const int tile = (int)(item / ld), c = (int)(item % ld);
+    const int a0 = tile * E;
+    T hv[E][kHist];
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+      for (int k = 0; k < kHist; ++k)
+        hv[e][k] = (k < nsteps && a0 + e < nA) ? P.hist[((size_t)k * nA + a0 + e) * ld + c] : T(0);
+    T w0[E];
+    if (first) {
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        w0[e] = (a0 + e < nA && c < P.R) ? (T)__ldg(P.W + (size_t)__ldg(P.active + a0 + e) * P.ldw + c) : T(0);
+    }
+    for (int j = 0; j < p; ++j) {
+      const bool on = P.pflag[j * ld + c] != 0 && nsteps > 0;
+      if (!first && !final_pass && !on) continue;
+      const size_t base = ((size_t)j * nA + a0) * ld + c;
+      T x[E], pv[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const bool ok = a0 + e < nA;
+        x[e] = first ? T(0) : (ok ? P.Xb[base + (size_t)e * ld] : T(0));
+        pv[e] = first ? w0[e] : ((on && ok) ? P.Pb[base + (size_t)e * ld] : T(0));
+      }
+      if (on) {
+#pragma unroll
+        for (int k = 0; k < kHist; ++k) {
+          if (k < nsteps) {
+            const size_t ci = ((size_t)k * p + j) * ld + c;
+            const T aj = P.ca[ci], zn = P.cz[ci], bj = P.cb[ci];
+            if (aj != T(0) || zn != T(0)) {
+#pragma unroll
+              for (int e = 0; e < E; ++e) {
+                x[e] = fma(aj, pv[e], x[e]);
+                pv[e] = fma(zn, hv[e][k], bj * pv[e]);
+              }
+            }
+          }
+        }
+        if (!final_pass) {
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+            if (a0 + e < nA) P.Pb[base + (size_t)e * ld] = pv[e];
+        }
+      }
+      if (final_pass) {
+        if (c < P.R) {
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            if (a0 + e < nA) {
+              const size_t o = ((size_t)j * nA + a0 + e) * P.ldx + c;
+              if (P.x_f32) reinterpret_cast<float*>(P.Xout)[o] = (float)x[e];
+              else reinterpret_cast<double*>(P.Xout)[o] = (double)x[e];
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (a0 + e < nA) P.Xb[base + (size_t)e * ld] = x[e];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+template <typename T, int VEC, bool WEIGHTED, int E>
+__global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
+  __shared__ double red[kWarps * kMaxLd];
+  __shared__ double s_col[2][kMaxLd];
+
+  GridSync gs;
+  gs.count = reinterpret_cast<unsigned*>(P.ctl + 4);
+  gs.gen = reinterpret_cast<unsigned*>(P.ctl + 5);
+  gs.err = P.ctl + 1;
+  gs.where = P.ctl + 2;
+  gs.timeout_ns = P.timeout_ns;
+
+  const int ld = P.ld, p = P.p, n = P.n, nA = P.nA;
+  const RowGroup rg = make_row_group<VEC>(ld);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gpw = 32 / rg.G;
+  const int gid = (blockIdx.x * kWarps + warp) * gpw + lane / rg.G;
+  const int GT = gridDim.x * kWarps * gpw;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  const long long nvec = (long long)n * rg.G;  // VEC-vectors in an n x ld block
+  double* my_part = P.part + (size_t)blockIdx.x * ld;
+
+  // ---- P0: r = d = W, partial r.r ----
+  {
+    double acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
+    for (long long e = tid; e < nvec; e += nth) {
+      const long long i = e / rg.G;
+      T w[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        const int c = rg.col + v;
+        w[v] = (c < P.R) ? (T)__ldg(P.W + (size_t)i * P.ldw + c) : T(0);
+        acc[v] += (double)w[v] * (double)w[v];
+      }
+      vstore<T, VEC>(P.r + (size_t)i * ld + rg.col, w);
+      vstore<T, VEC>(P.d + (size_t)i * ld + rg.col, w);
+    }
+    reduce_cols_to_part<VEC>(acc, rg.G, ld, red, my_part);
+  }
+  {
+    unsigned g0;
+    if (grid_arrive(gs, g0)) {
+      reduce_partials(P.part, gridDim.x, ld, red, s_col[0]);
+      int anyv = 0;
+      for (int c = threadIdx.x; c < ld; c += blockDim.x) {
+        const double rr = s_col[0][c];
+        if (!isfinite(rr)) atomicCAS(P.ctl + 1, 0, (int)POLAR_ERR_NONFINITE);
+        const int a = rr > 0.0 ? 1 : 0;
+        P.rr[c] = rr;
+        P.stop[c] = P.tol * sqrt(rr);
+        P.act[c] = a;
+        P.upd[c] = 0;
+        P.ap[c] = 1.0;
+        P.bp[c] = 0.0;
+        P.ag[c] = 0.0;
+        P.beg[c] = 0.0;
+        P.chig[c] = 0.0;
+        anyv |= a;
+      }
+      for (int it = threadIdx.x; it < p * ld; it += blockDim.x) {
+        const int c = it % ld;
+        const double rr = s_col[0][c];
+        P.z[it] = 1.0;
+        P.zp[it] = 1.0;
+        P.live[it] = rr > 0.0 ? 1 : 0;
+        P.hs[it] = 0.0;
+        P.ip[it] = 0.0;
+        P.pn[it] = rr;
+        P.pflag[it] = 0;
+      }
+      anyv = __syncthreads_or(anyv);
+      if (threadIdx.x == 0) {
+        P.ctl[3] = anyv;
+        P.stats[0] = 0;
+        P.stats[1] = 0;
+      }
+      if (!grid_release(gs, g0)) return;
+    } else if (!grid_wait(gs, g0, 1)) {
+      return;
+    }
+  }
+
+  const double shift0 = __ldg(P.tau);
+  const int lgG = __ffs(rg.G) - 1;
+  int pending = 0;
+  bool first = true;
+  bool flush_pending = false;
+  long long it = 0;
+  bool capped = false;
+  bool more = ld_volatile_i32(P.ctl + 3) != 0 && P.maxit > 0;
+  if (ld_volatile_i32(P.ctl + 3) != 0 && P.maxit <= 0) capped = true;
+  while (more) {
+    // ---- P4 (deferred shifted update of the previous M iterations) ----
+    if (flush_pending) {
+      shifted_update<T, E>(P, pending, first, false, tid, nth);
+      first = false;
+      pending = 0;
+      flush_pending = false;
+      if (blockIdx.x == 0 && threadIdx.x == 0) P.stats[1] += 1;
+    }
+    // ---- P1 ----
+    {
+      double dacc[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dacc[v] = 0.0;
+      spmm_phase<T, VEC, WEIGHTED>(P.g, rg, gid, GT, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, dacc);
+      reduce_cols_to_part<VEC>(dacc, rg.G, ld, red, my_part);
+    }
+    // ---- R1 ----
+    {
+      unsigned g1;
+      if (grid_arrive(gs, g1)) {
+        reduce_partials(P.part, gridDim.x, ld, red, s_col[0]);
+        for (int c = threadIdx.x; c < ld; c += blockDim.x) {
+          const int a_on = P.act[c];
+          const double dv = s_col[0][c];
+          const double a = a_on ? P.rr[c] / dv : 0.0;
+          if (a_on && !isfinite(a)) atomicCAS(P.ctl + 1, 0, (int)POLAR_ERR_NONFINITE);
+          P.ag[c] = a;
+        }
+        if (!grid_release(gs, g1)) return;
+      } else if (!grid_wait(gs, g1, 2)) {
+        return;
+      }
+    }
+    // ---- P2 ----
+    {
+      double a_c[VEC], racc[VEC];
+      bool on[VEC], any_on = false;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        a_c[v] = P.ag[rg.col + v];
+        on[v] = P.act[rg.col + v] != 0;
+        any_on |= on[v];
+        racc[v] = 0.0;
+      }
+      if (any_on) {
+        T* hslot = P.hist + (size_t)pending * nA * ld;
+        constexpr int U = 2;
+        for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
+          T rv[U][VEC], vv[U][VEC];
+          long long ii[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const long long e = e0 + u * nth;
+            ii[u] = e < nvec ? (e >> lgG) : -1;
+            if (ii[u] >= 0) {
+              vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+              vload<T, VEC>(vv[u], P.v + (size_t)ii[u] * ld + rg.col);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (ii[u] < 0) continue;
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) {
+              if (on[v]) rv[u][v] = (T)((double)rv[u][v] - a_c[v] * (double)vv[u][v]);
+              racc[v] += (double)rv[u][v] * (double)rv[u][v];
+            }
+            vstore<T, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
+            const int ai = __ldg(P.active_pos + ii[u]);
+            if (ai >= 0) vstore<T, VEC>(hslot + (size_t)ai * ld + rg.col, rv[u]);
+          }
+        }
+      }
+      reduce_cols_to_part<VEC>(racc, rg.G, ld, red, my_part);
+    }
+    // ---- R2: column scalars (serial, last CTA) ----
+    {
+      unsigned g2;
+      if (grid_arrive(gs, g2)) {
+        double* s_rrn = s_col[0];
+        reduce_partials(P.part, gridDim.x, ld, red, s_rrn);
+        int anyv2 = 0;
+        for (int c = threadIdx.x; c < ld; c += blockDim.x) {
+          const int a_on = P.act[c];
+          const double rrn = s_rrn[c];
+          const double a = P.ag[c];
+          const double rr = P.rr[c];
+          const double be = a_on ? rrn / rr : 0.0;
+          P.chig[c] = a_on ? a * P.bp[c] / P.ap[c] : 0.0;
+          P.upd[c] = a_on;
+          P.beg[c] = be;
+          if (a_on) {
+            if (!isfinite(rrn)) atomicCAS(P.ctl + 1, 0, (int)POLAR_ERR_NONFINITE);
+            P.rr[c] = rrn;
+            P.ap[c] = a;
+            P.bp[c] = be;
+            const bool done = sqrt(rrn) <= P.stop[c];
+            P.act[c] = done ? 0 : 1;
+            anyv2 |= done ? 0 : 1;
+            if (c < P.R) P.iters_out[c] += 1;
+          }
+        }
+        anyv2 = __syncthreads_or(anyv2);
+        if (threadIdx.x == 0) {
+          P.ctl[3] = anyv2;
+          P.stats[0] = it + 1;
+        }
+        if (!grid_release(gs, g2)) return;
+      } else if (!grid_wait(gs, g2, 3)) {
+        return;
+      }
+    }
+    const int any_after = ld_volatile_i32(P.ctl + 3);
+    more = any_after && it + 1 < P.maxit;
+    capped = any_after && !more;
+    // ---- pole recurrences (distributed: each thread owns fixed (pole, column) items) ----
+    for (long long q = tid; q < (long long)p * ld; q += nth) {
+      const int j = (int)(q / ld), c = (int)(q % ld);
+      const bool m = P.live[q] && P.upd[c];
+      const size_t ci = ((size_t)pending * p + j) * ld + c;
+      int pf = pending == 0 ? 0 : P.pflag[q];
+      if (m) {
+        const double theta = __ldg(P.tau + j) - shift0;
+        const double a = P.ag[c], be = P.beg[c], chi = P.chig[c], rrn = P.rr[c];
+        const double z = P.z[q], zp = P.zp[q];
+        const double zn = z / (1.0 + a * theta + chi * (1.0 - z / zp));
+        const double fac = zn / z;
+        const double aj = a * fac;
+        const double bj = be * fac * fac;
+        P.ca[ci] = (T)aj;
+        P.cz[ci] = (T)zn;
+        P.cb[ci] = (T)bj;
+        if (P.track) {
+          const double ipv = P.ip[q], pnv = P.pn[q];
+          P.hs[q] += 2.0 * aj * ipv + aj * aj * pnv;
+          P.ip[q] = bj * (ipv + aj * pnv);
+          P.pn[q] = zn * zn * rrn + bj * bj * pnv;
+        }
+        P.zp[q] = z;
+        P.z[q] = zn;
+        if (fabs(zn) * sqrt(rrn) <= P.stop[c]) P.live[q] = 0;
+        pf = 1;
+      } else {
+        P.ca[ci] = T(0);
+        P.cz[ci] = T(0);
+        P.cb[ci] = T(1);
+      }
+      P.pflag[q] = pf;
+    }
+    // ---- P3 ----
+    if (more) {
+      double be_c[VEC];
+      bool on[VEC], any_on = false;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) {
+        be_c[v] = P.beg[rg.col + v];
+        on[v] = P.upd[rg.col + v] != 0;
+        any_on |= on[v];
+      }
+      if (any_on) {
+        constexpr int U = 2;
+        for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
+          T rv[U][VEC], dv[U][VEC];
+          long long ii[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const long long e = e0 + u * nth;
+            ii[u] = e < nvec ? (e >> lgG) : -1;
+            if (ii[u] >= 0) {
+              vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+              vload<T, VEC>(dv[u], P.d + (size_t)ii[u] * ld + rg.col);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (ii[u] < 0) continue;
+#pragma unroll
+            for (int v = 0; v < VEC; ++v)
+              if (on[v]) dv[u][v] = (T)((double)rv[u][v] + be_c[v] * (double)dv[u][v]);
+            vstore<T, VEC>(P.d + (size_t)ii[u] * ld + rg.col, dv[u]);
+          }
+        }
+      }
+    }
+    ++pending;
+    ++it;
+    flush_pending = pending == kHist;
+    if (!grid_sync(gs, 4)) return;
+  }
+  // ---- final pass: remaining steps, X -> output ----
+  shifted_update<T, E>(P, pending, first, true, tid, nth);
+  if (blockIdx.x == 0) {
+    if (P.track && P.h_out)
+      for (int q = threadIdx.x; q < p * ld; q += blockDim.x) {
+        const int j = q / ld, c = q % ld;
+        if (c < P.R) P.h_out[(size_t)j * P.R + c] = P.hs[q];
+      }
+    if (threadIdx.x == 0) {
+      P.stats[1] += 1;
+      P.ctl[0] = capped ? (int)POLAR_ERR_ITER_CAP : 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+struct SolveLayout {
+  size_t off[40];
+  size_t total;
+  int ld, vec;
+};
+
+static int choose_vec(int precision, int ld) {
+  if (precision == POLAR_MIXED) return ld >= 4 ? 4 : ld;
+  return ld >= 2 ? 2 : 1;
+}
+
+static int choose_ld(int precision, int R) {
+  int ld = next_pow2(R < 1 ? 1 : R);
+  const int vec = choose_vec(precision, ld);
+  if (ld < vec) ld = vec;
+  return ld;
+}
+
+static int max_ld(int precision) { return precision == POLAR_MIXED ? 128 : 64; }
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+static int max_grid_for(int precision, int vec, bool weighted);
+
+static void solve_layout(const polar_graph* g, int precision, int R, int p, int nA, int grid, SolveLayout* L) {
+  const int ld = choose_ld(precision, R);
+  const size_t ts = precision == POLAR_MIXED ? 4 : 8;
+  const size_t n = g->n;
+  size_t o = 0;
+  int k = 0;
+  auto add = [&](size_t bytes) {
+    L->off[k++] = o;
+    o += align256(bytes);
+  };
+  add(n * ld * ts);                                // 0 r
+  add(n * ld * ts);                                // 1 d
+  add(n * ld * ts);                                // 2 v
+  add((size_t)kHist * nA * ld * ts);               // 3 hist
+  add((size_t)p * nA * ld * ts);                   // 4 P
+  add((size_t)p * nA * ld * ts);                   // 5 X
+  add((size_t)(g->nchunks > 0 ? g->nchunks : 1) * ld * ts);  // 6 chunk partials
+  add((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4);           // 7 heavy counters
+  add((size_t)grid * ld * 8);                      // 8 CTA partials
+  for (int i = 0; i < 6; ++i) add((size_t)ld * 8);  // 9..14 rr stop ap bp a be
+  add((size_t)ld * 4);                             // 15 act
+  add((size_t)ld * 4);                             // 16 upd
+  for (int i = 0; i < 5; ++i) add((size_t)p * ld * 8);  // 17..21 z zp h ip pn
+  add((size_t)p * ld * 4);                         // 22 live
+  add((size_t)p * ld * 4);                         // 23 pflag
+  for (int i = 0; i < 3; ++i) add((size_t)kHist * p * ld * ts);  // 24..26 coef planes
+  add(64);                                         // 27 ctl
+  add(64);                                         // 28 stats
+  add((size_t)ld * 8);                             // 29 chi
+  L->total = o;
+  L->ld = ld;
+  L->vec = choose_vec(precision, ld);
+}
+
+template <typename T, int VEC, bool WEIGHTED, int E>
+static int launch_solve(const SolvePrm<T>& prm, int grid, cudaStream_t st) {
+  void* args[] = {(void*)&prm};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)msolve_kernel<T, VEC, WEIGHTED, E>, dim3(grid),
+                                              dim3(kBlock), args, 0, st);
+  if (e != cudaSuccess) return set_cuda_error("cudaLaunchCooperativeKernel(msolve)", e);
+  return POLAR_OK;
+}
+
+template <typename T, int VEC, bool WEIGHTED, int E>
+static int occupancy_of() {
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, msolve_kernel<T, VEC, WEIGHTED, E>, kBlock, 0);
+  return nb;
+}
+
+static int max_grid_for(int precision, int vec, bool weighted) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int nb = 0;
+  if (precision == POLAR_MIXED) {
+    if (vec == 4) nb = weighted ? occupancy_of<float, 4, true, 4>() : occupancy_of<float, 4, false, 4>();
+    else if (vec == 2) nb = weighted ? occupancy_of<float, 2, true, 4>() : occupancy_of<float, 2, false, 4>();
+    else nb = weighted ? occupancy_of<float, 1, true, 4>() : occupancy_of<float, 1, false, 4>();
+  } else {
+    if (vec == 2) nb = weighted ? occupancy_of<double, 2, true, 2>() : occupancy_of<double, 2, false, 2>();
+    else nb = weighted ? occupancy_of<double, 1, true, 2>() : occupancy_of<double, 1, false, 2>();
+  }
+  if (nb < 1) nb = 1;
+  return nb * sms;
+}
+
+static uint64_t g_timeout_ns = 4000000000ull;  // 4 s per barrier wait
+
+}  // namespace polar
+
+using namespace polar;
+
+extern "C" void polar_set_barrier_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 1; }
+
+extern "C" size_t polar_msolve_workspace_bytes(const polar_graph* g, int precision, int R, int p, int nA) {
+  if (!g || R < 1 || p < 1 || nA < 0) return 0;
+  const int ld = choose_ld(precision, R);
+  SolveLayout L;
+  solve_layout(g, precision, R, p, nA, max_grid_for(precision, choose_vec(precision, ld), g->d_wts != nullptr), &L);
+  return L.total;
+}
+
+extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d_W, int ldw, int R,
+                            const double* d_tau, int p, const int32_t* d_active, const int32_t* d_active_pos,
+                            int nA, double tol, int64_t maxit, int track, void* d_X_out, int x_f32, int ldx,
+                            double* d_h_out, int64_t* d_iters_out, void* d_workspace, size_t workspace_bytes,
+                            polar_stream_t stream) {
+  clear_error();
+  if (!g || !d_W || !d_tau || !d_X_out || !d_iters_out || !d_workspace) return set_error(POLAR_ERR_BAD_ARG, "null pointer");
+  if (precision != POLAR_FP64 && precision != POLAR_MIXED) return set_error(POLAR_ERR_BAD_ARG, "precision");
+  if (R < 1 || R > max_ld(precision)) return set_error(POLAR_ERR_BAD_ARG, "R out of range for this precision");
+  if (p < 1 || nA < 1 || ldw < R || ldx < R || g->n < 1) return set_error(POLAR_ERR_BAD_ARG, "bad sizes");
+  if (track && !d_h_out) return set_error(POLAR_ERR_BAD_ARG, "track needs h_out");
+  if ((g->d_wts == nullptr) != (g->d_diag == nullptr)) return set_error(POLAR_ERR_BAD_ARG, "weights and diag go together");
+  const int ld = choose_ld(precision, R);
+  const int vec = choose_vec(precision, ld);
+  const bool weighted = g->d_wts != nullptr;
+  const int grid = max_grid_for(precision, vec, weighted);
+  SolveLayout L;
+  solve_layout(g, precision, R, p, nA, grid, &L);
+  if (workspace_bytes < L.total) return set_error(POLAR_ERR_WORKSPACE, "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)d_workspace;
+  // zero the small control/state regions the kernel expects cleared
+  cudaError_t e;
+  e = cudaMemsetAsync(ws + L.off[27], 0, 64, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws + L.off[28], 0, 64, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws + L.off[7], 0, align256((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_iters_out, 0, sizeof(int64_t) * R, st);
+  if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync", e);
+
+  auto fill = [&](auto* prm_ptr) {
+    auto& prm = *prm_ptr;
+    using TT = std::remove_pointer_t<decltype(prm.r)>;
+    prm.g = *g;
+    prm.n = g->n;
+    prm.R = R;
+    prm.ld = ld;
+    prm.p = p;
+    prm.nA = nA;
+    prm.tol = tol;
+    prm.maxit = maxit;
+    prm.track = track;
+    prm.W = d_W;
+    prm.ldw = ldw;
+    prm.tau = d_tau;
+    prm.active = d_active;
+    prm.active_pos = d_active_pos;
+    prm.Xout = d_X_out;
+    prm.x_f32 = x_f32;
+    prm.ldx = ldx;
+    prm.h_out = d_h_out;
+    prm.iters_out = (long long*)d_iters_out;
+    prm.r = (TT*)(ws + L.off[0]);
+    prm.d = (TT*)(ws + L.off[1]);
+    prm.v = (TT*)(ws + L.off[2]);
+    prm.hist = (TT*)(ws + L.off[3]);
+    prm.Pb = (TT*)(ws + L.off[4]);
+    prm.Xb = (TT*)(ws + L.off[5]);
+    prm.chunk_part = (TT*)(ws + L.off[6]);
+    prm.hcount = (int*)(ws + L.off[7]);
+    prm.part = (double*)(ws + L.off[8]);
+    prm.rr = (double*)(ws + L.off[9]);
+    prm.stop = (double*)(ws + L.off[10]);
+    prm.ap = (double*)(ws + L.off[11]);
+    prm.bp = (double*)(ws + L.off[12]);
+    prm.ag = (double*)(ws + L.off[13]);
+    prm.beg = (double*)(ws + L.off[14]);
+    prm.act = (int*)(ws + L.off[15]);
+    prm.upd = (int*)(ws + L.off[16]);
+    prm.z = (double*)(ws + L.off[17]);
+    prm.zp = (double*)(ws + L.off[18]);
+    prm.hs = (double*)(ws + L.off[19]);
+    prm.ip = (double*)(ws + L.off[20]);
+    prm.pn = (double*)(ws + L.off[21]);
+    prm.live = (int*)(ws + L.off[22]);
+    prm.pflag = (int*)(ws + L.off[23]);
+    prm.ca = (TT*)(ws + L.off[24]);
+    prm.cz = (TT*)(ws + L.off[25]);
+    prm.cb = (TT*)(ws + L.off[26]);
+    prm.ctl = (int*)(ws + L.off[27]);
+    prm.stats = (long long*)(ws + L.off[28]);
+    prm.chig = (double*)(ws + L.off[29]);
+    prm.timeout_ns = g_timeout_ns;
+  };
+  int rc;
+  if (precision == POLAR_MIXED) {
+    SolvePrm<float> prm;
+    fill(&prm);
+    if (vec == 4) rc = weighted ? launch_solve<float, 4, true, 4>(prm, grid, st) : launch_solve<float, 4, false, 4>(prm, grid, st);
+    else if (vec == 2) rc = weighted ? launch_solve<float, 2, true, 4>(prm, grid, st) : launch_solve<float, 2, false, 4>(prm, grid, st);
+    else rc = weighted ? launch_solve<float, 1, true, 4>(prm, grid, st) : launch_solve<float, 1, false, 4>(prm, grid, st);
+  } else {
+    SolvePrm<double> prm;
+    fill(&prm);
+    if (vec == 2) rc = weighted ? launch_solve<double, 2, true, 2>(prm, grid, st) : launch_solve<double, 2, false, 2>(prm, grid, st);
+    else rc = weighted ? launch_solve<double, 1, true, 2>(prm, grid, st) : launch_solve<double, 1, false, 2>(prm, grid, st);
+  }
+  if (rc != POLAR_OK) return rc;
+  // remember the control block location for polar_msolve_finish
+  remember_solve(d_workspace, (int*)(ws + L.off[27]), (long long*)(ws + L.off[28]), ld, grid, kBlock);
+  return POLAR_OK;
+}
+
+extern "C" int polar_msolve_finish(void* d_workspace, polar_stream_t stream, polar_msolve_info* info) {
+  clear_error();
+  SolveRecord rec;
+  if (!lookup_solve(d_workspace, &rec)) return set_error(POLAR_ERR_BAD_ARG, "no solve launched on this workspace");
+  int ctl[4];
+  long long stats[2];
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(ctl, rec.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(stats, rec.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_cuda_error("msolve finish", e);
+  int status = ctl[1] != 0 ? ctl[1] : ctl[0];
+  if (info) {
+    info->status = status;
+    info->ld = rec.ld;
+    info->grid = rec.grid;
+    info->block = rec.block;
+    info->iterations = stats[0];
+    info->flushes = stats[1];
+    info->error_where = ctl[2];
+    info->pad = 0;
+  }
+  if (status == POLAR_ERR_ITER_CAP) return set_error(status, "multi-shift CG iteration cap");
+  if (status == POLAR_ERR_NONFINITE) return set_error(status, "non-finite value in CG");
+  if (status == POLAR_ERR_TIMEOUT) return set_error(status, "grid barrier wait timed out");
+  return status;
+}

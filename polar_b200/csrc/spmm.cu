@@ -1,0 +1,157 @@
+// Standalone operator apply: Y = (M + shift I) X  (realworld/spmm.py:4-25, polar_gpu.py:71-80).
+//
+// The same row-group SpMM as the solver's P1 phase, as an ordinary launch.  Heavy rows
+// are split into chunks whose partial sums are combined by the last chunk to finish, in
+// chunk order, so the result does not depend on scheduling.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "graph_ops.cuh"
+#include "host_util.h"
+
+namespace polar {
+
+constexpr int kSpmmBlock = 256;
+
+template <typename T, int VEC, bool WEIGHTED>
+__global__ void __launch_bounds__(kSpmmBlock) spmm_kernel(polar_graph g, int R, int G, double shift, const T* X,
+                                                          int ldx, T* Y, int ldy,
+                                                          typename AccOf<T>::type* part, int* hcount) {
+  using A = typename AccOf<T>::type;
+  RowGroup rg;
+  rg.G = G;
+  const int lane = threadIdx.x & 31;
+  rg.lg = lane & (G - 1);
+  const int base = lane - rg.lg;
+  rg.mask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << base);
+  rg.col = rg.lg * VEC;
+  const bool on = rg.col < R;
+  if (!on) rg.col = 0;  // idle lanes still take part in the index shuffles
+  const int gpw = 32 / G;
+  const int gid = (blockIdx.x * (kSpmmBlock / 32) + (threadIdx.x >> 5)) * gpw + lane / G;
+  const int GT = gridDim.x * (kSpmmBlock / 32) * gpw;
+  const int ldp = G * VEC;
+
+  for (int ch = gid; ch < g.nchunks; ch += GT) {
+    const int h = g.d_chunk_row[ch];
+    A acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, g.d_chunk_lo[ch], g.d_chunk_hi[ch], X, ldx, acc);
+    vstore<A, VEC>(part + (size_t)ch * ldp + rg.lg * VEC, acc);
+    __threadfence();
+    __syncwarp(rg.mask);
+    int old = 0;
+    if (rg.lg == 0) old = atomicAdd(hcount + h, 1);
+    old = __shfl_sync(rg.mask, old, 0, G);
+    const int c0 = g.d_hchunk_off[h], c1 = g.d_hchunk_off[h + 1];
+    if (old == c1 - c0 - 1) {
+      __threadfence();
+      A sum[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) sum[v] = A(0);
+      for (int c2 = c0; c2 < c1; ++c2) {
+        A pv[VEC];
+        vload_cg<A, VEC>(pv, part + (size_t)c2 * ldp + rg.lg * VEC);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
+      }
+      const int i = g.d_hrow[h];
+      T xi[VEC], yi[VEC];
+      finish_row<T, VEC>(g, rg, i, g.d_indptr[i + 1] - g.d_indptr[i], shift, X, ldx, sum, Y, ldy, xi, yi, on);
+      if (rg.lg == 0) hcount[h] = 0;
+    }
+  }
+  for (int i = gid; i < g.n; i += GT) {
+    const int lo = g.d_indptr[i], hi = g.d_indptr[i + 1];
+    if (hi - lo > g.heavy_thresh) continue;
+    A acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ldx, acc);
+    T xi[VEC], yi[VEC];
+    finish_row<T, VEC>(g, rg, i, hi - lo, shift, X, ldx, acc, Y, ldy, xi, yi, on);
+  }
+}
+
+static int spmm_vec(int precision, int R, int ldx, int ldy, const void* X, const void* Y) {
+  const int maxv = precision == POLAR_MIXED ? 4 : 2;
+  const size_t es = precision == POLAR_MIXED ? 4 : 8;
+  for (int v = maxv; v > 1; v >>= 1) {
+    if (R % v == 0 && ldx % v == 0 && ldy % v == 0 && ((uintptr_t)X % (v * es)) == 0 &&
+        ((uintptr_t)Y % (v * es)) == 0)
+      return v;
+  }
+  return 1;
+}
+
+template <typename T, int VEC, bool W>
+static int launch_spmm(const polar_graph& g, int R, double shift, const void* X, int ldx, void* Y, int ldy,
+                       void* scratch, cudaStream_t st) {
+  using A = typename AccOf<T>::type;
+  const int G = next_pow2((R + VEC - 1) / VEC);
+  const int ldp = G * VEC;
+  A* part = reinterpret_cast<A*>(scratch);
+  int* hcount = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) +
+                                       (((size_t)(g.nchunks > 0 ? g.nchunks : 1) * 128 * sizeof(A) + 255) & ~size_t(255)));
+  (void)ldp;
+  const int gpb = (kSpmmBlock / 32) * (32 / G);
+  long long groups_needed = (long long)g.n + g.nchunks;
+  long long blocks = (groups_needed + gpb - 1) / gpb;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long cap = (long long)sms * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  spmm_kernel<T, VEC, W><<<(int)blocks, kSpmmBlock, 0, st>>>(g, R, G, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error("spmm launch", e);
+  return POLAR_OK;
+}
+
+}  // namespace polar
+
+using namespace polar;
+
+extern "C" size_t polar_spmm_scratch_bytes(const polar_graph* g, int precision, int R) {
+  (void)R;
+  if (!g) return 0;
+  const size_t es = precision == POLAR_MIXED ? 4 : 8;
+  const size_t part = (((size_t)(g->nchunks > 0 ? g->nchunks : 1) * 128 * es + 255) & ~size_t(255));
+  return part + (((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 + 255) & ~size_t(255));
+}
+
+extern "C" int polar_spmm_scratch_init(const polar_graph* g, int precision, int R, void* d_scratch,
+                                       polar_stream_t stream) {
+  clear_error();
+  if (!g || !d_scratch) return set_error(POLAR_ERR_BAD_ARG, "null pointer");
+  cudaError_t e = cudaMemsetAsync(d_scratch, 0, polar_spmm_scratch_bytes(g, precision, R), (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync", e);
+  return POLAR_OK;
+}
+
+extern "C" int polar_spmm(const polar_graph* g, int precision, int R, double shift, const void* d_X, int ldx,
+                          void* d_Y, int ldy, void* d_scratch, polar_stream_t stream) {
+  clear_error();
+  if (!g || !d_X || !d_Y || !d_scratch) return set_error(POLAR_ERR_BAD_ARG, "null pointer");
+  if (R < 1 || ldx < R || ldy < R) return set_error(POLAR_ERR_BAD_ARG, "bad sizes");
+  const int vec = spmm_vec(precision, R, ldx, ldy, d_X, d_Y);
+  if ((R + vec - 1) / vec > 32) return set_error(POLAR_ERR_BAD_ARG, "R too large for one pass; split columns");
+  if ((g->d_wts == nullptr) != (g->d_diag == nullptr)) return set_error(POLAR_ERR_BAD_ARG, "weights and diag go together");
+  const bool w = g->d_wts != nullptr;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (precision == POLAR_MIXED) {
+    if (vec == 4) return w ? launch_spmm<float, 4, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+                           : launch_spmm<float, 4, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
+    if (vec == 2) return w ? launch_spmm<float, 2, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+                           : launch_spmm<float, 2, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
+    return w ? launch_spmm<float, 1, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+             : launch_spmm<float, 1, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
+  }
+  if (precision != POLAR_FP64) return set_error(POLAR_ERR_BAD_ARG, "precision");
+  if (vec == 2) return w ? launch_spmm<double, 2, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+                         : launch_spmm<double, 2, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
+  return w ? launch_spmm<double, 1, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+           : launch_spmm<double, 1, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
+}

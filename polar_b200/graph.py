@@ -1,0 +1,256 @@
+"""Graph operator on the device: M0 = L + sigma I as a CSR of neighbour lists, and the
+operator view Op = M0 + sum_S w b b^T (+ shift I) used by the solver.
+
+Mirrors realworld/polar_gpu.py:47-80 (Graph, Op).  Layout in HBM:
+* indptr int32[n+1], indices int32[nnz] (off-diagonal neighbours only, sorted per row);
+  unweighted graphs store no values (weight 1, diagonal = degree + sigma);
+* weighted graphs add wts float64[nnz] and diag float64[n];
+* rows with more than `heavy_thresh` neighbours are split into chunks of that size
+  (hrow, hchunk_off, chunk_row/lo/hi), combined in a fixed order by the kernels;
+* edges added by Op.add live in a small side structure (bitset over rows + sorted row
+  list + neighbour lists), so the CSR is never rebuilt during the greedy.
+"""
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from . import _lib
+
+__all__ = ["Graph", "Op", "default_device"]
+
+
+def default_device():
+    """The current CUDA device; Graph(device='cpu') builds the host structures only
+    (for tests of the host logic), and no kernel can run on it."""
+    if not torch.cuda.is_available():
+        raise RuntimeError("polar_b200 needs a CUDA device (B200, sm_100a); none is available")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _i32(x, dev):
+    return torch.as_tensor(np.ascontiguousarray(x, dtype=np.int32)).to(dev)
+
+
+class _HostM0:
+    """Host FP64 CSR of M0 = diag(deg + sigma) - A with the `.get()` the drivers call
+    (realworld/run_real.py:49 uses G.M0.get().toarray() for dense oracles)."""
+
+    def __init__(self, G):
+        self._G = G
+        self._csr = None
+
+    def get(self):
+        if self._csr is None:
+            G = self._G
+            A = sp.csr_matrix((G._data_h, G._indices_h, G._indptr_h), shape=(G.n, G.n))
+            M = (sp.diags(G._deg_h + G.sigma) - A).tocsr()
+            M.sort_indices()
+            self._csr = M
+        return self._csr
+
+    @property
+    def shape(self):
+        return (self._G.n, self._G.n)
+
+
+class Graph:
+    """Graph(n, edges, sigma, weights=None): realworld/polar_gpu.py:47-60.
+
+    Attributes as in the reference: n, sigma, M0 (host CSR via .get()), dmax, m, edges,
+    weights; plus the device CSR used by the kernels."""
+
+    def __init__(self, n, edges, sigma, weights=None, *, heavy_thresh=256, device=None):
+        self.n = int(n)
+        self.sigma = float(sigma)
+        self.device = default_device() if device is None else torch.device(device)
+        edges = np.asarray(edges, dtype=np.int64).reshape(-1, 2)
+        u, v = edges[:, 0], edges[:, 1]
+        if len(u) and (u.min() < 0 or v.min() < 0 or max(u.max(), v.max()) >= self.n):
+            raise ValueError("edge endpoint out of range")
+        w = np.ones(len(u)) if weights is None else np.asarray(weights, np.float64)
+        if len(w) != len(u):
+            raise ValueError("weights must match edges")
+        deg = np.bincount(u, w, self.n) + np.bincount(v, w, self.n)
+        A = sp.csr_matrix((np.r_[w, w], (np.r_[u, v], np.r_[v, u])), shape=(self.n, self.n))
+        A.sum_duplicates()
+        A.sort_indices()
+        if A.nnz >= 2 ** 31:
+            raise ValueError("graph too large for int32 CSR")
+        self.dmax = float(deg.max()) if self.n else 0.0
+        self.m = len(u)
+        self.edges = edges
+        self.weights = w
+        self.M0 = _HostM0(self)
+        self._indptr_h = A.indptr.astype(np.int32)
+        self._indices_h = A.indices.astype(np.int32)
+        self._data_h = A.data
+        self._deg_h = deg
+        self.nnz = int(A.nnz)
+        self.weighted = weights is not None and not np.all(self._data_h == 1.0)
+        dev = self.device
+        self.indptr = _i32(self._indptr_h, dev)
+        self.indices = _i32(self._indices_h, dev)
+        if self.weighted:
+            self.wts = torch.as_tensor(self._data_h, dtype=torch.float64).to(dev)
+            self.diag = torch.as_tensor(deg + self.sigma, dtype=torch.float64).to(dev)
+        else:
+            self.wts = None
+            self.diag = None
+        self._split_heavy(int(heavy_thresh))
+
+    # -- heavy-row split ---------------------------------------------------------------
+    def _split_heavy(self, thresh):
+        self.heavy_thresh = max(1, thresh)
+        degs = np.diff(self._indptr_h.astype(np.int64))
+        hrow = np.flatnonzero(degs > self.heavy_thresh).astype(np.int32)
+        nch = -(-degs[hrow] // self.heavy_thresh) if len(hrow) else np.zeros(0, np.int64)
+        off = np.zeros(len(hrow) + 1, np.int64)
+        off[1:] = np.cumsum(nch)
+        total = int(off[-1])
+        chunk_row = np.repeat(np.arange(len(hrow), dtype=np.int32), nch)
+        within = np.arange(total, dtype=np.int64) - np.repeat(off[:-1], nch)
+        lo = self._indptr_h[hrow].astype(np.int64)
+        hi = self._indptr_h[hrow + 1].astype(np.int64) if len(hrow) else np.zeros(0, np.int64)
+        c_lo = np.repeat(lo, nch) + within * self.heavy_thresh
+        c_hi = np.minimum(c_lo + self.heavy_thresh, np.repeat(hi, nch))
+        dev = self.device
+        self.nheavy = len(hrow)
+        self.nchunks = total
+        one = np.zeros(1, np.int32)
+        self.hrow = _i32(hrow if len(hrow) else one, dev)
+        self.hchunk_off = _i32(off, dev)
+        self.chunk_row = _i32(chunk_row if total else one, dev)
+        self.chunk_lo = _i32(c_lo if total else one, dev)
+        self.chunk_hi = _i32(c_hi if total else one, dev)
+
+    def Lam(self, k):
+        """Spectral upper bound sigma + 2 dmax + 4k (realworld/polar_gpu.py:59-60)."""
+        return self.sigma + 2.0 * self.dmax + 4.0 * k
+
+    def struct(self, extra=None):
+        """ctypes polar_graph for this graph (plus an Op's added edges)."""
+        s = _lib.PolarGraph()
+        s.n = self.n
+        s.nnz = self.nnz
+        s.d_indptr = self.indptr.data_ptr()
+        s.d_indices = self.indices.data_ptr() if self.nnz else self.indptr.data_ptr()
+        s.d_wts = self.wts.data_ptr() if self.weighted else None
+        s.d_diag = self.diag.data_ptr() if self.weighted else None
+        s.sigma = self.sigma
+        s.nx = 0
+        s.heavy_thresh = self.heavy_thresh
+        s.nheavy = self.nheavy
+        s.nchunks = self.nchunks
+        s.d_hrow = self.hrow.data_ptr()
+        s.d_hchunk_off = self.hchunk_off.data_ptr()
+        s.d_chunk_row = self.chunk_row.data_ptr()
+        s.d_chunk_lo = self.chunk_lo.data_ptr()
+        s.d_chunk_hi = self.chunk_hi.data_ptr()
+        if extra is not None:
+            extra.fill(s)
+        return s
+
+
+class _Added:
+    """Edges added during the greedy (Op.add), as the side structure the kernels read."""
+
+    def __init__(self, G):
+        self.G = G
+        self.nbr = {}       # row -> list of (neighbour, weight)
+        self.bits_h = np.zeros((G.n + 31) // 32, dtype=np.uint32)
+        self.bits_d = torch.zeros(len(self.bits_h), dtype=torch.int32, device=G.device)
+        self.dirty = False
+        self.weighted = False
+        self.rows_d = self.off_d = self.nbr_d = self.wt_d = None
+
+    def add(self, a, b, w):
+        for x, y in ((a, b), (b, a)):
+            self.nbr.setdefault(x, []).append((y, w))
+        if w != 1.0:
+            self.weighted = True
+        words = sorted({a >> 5, b >> 5})
+        for r in (a, b):
+            self.bits_h[r >> 5] |= np.uint32(1 << (r & 31))
+        idx = torch.as_tensor(np.array(words, dtype=np.int64), device=self.G.device)
+        vals = torch.as_tensor(self.bits_h[words].view(np.int32).copy(), device=self.G.device)
+        self.bits_d.index_copy_(0, idx, vals)
+        self.dirty = True
+
+    def _upload(self):
+        rows = np.array(sorted(self.nbr), dtype=np.int32)
+        off = np.zeros(len(rows) + 1, dtype=np.int32)
+        off[1:] = np.cumsum([len(self.nbr[r]) for r in rows])
+        nb = np.array([x for r in rows for x, _ in self.nbr[r]], dtype=np.int32)
+        wt = np.array([w for r in rows for _, w in self.nbr[r]], dtype=np.float64)
+        dev = self.G.device
+        self.rows_d = _i32(rows, dev)
+        self.off_d = _i32(off, dev)
+        self.nbr_d = _i32(nb, dev)
+        self.wt_d = torch.as_tensor(wt).to(dev) if self.weighted else None
+        self.dirty = False
+
+    def fill(self, s):
+        if not self.nbr:
+            return
+        if self.dirty:
+            self._upload()
+        s.nx = len(self.nbr)
+        s.d_xbits = self.bits_d.data_ptr()
+        s.d_xrow = self.rows_d.data_ptr()
+        s.d_xoff = self.off_d.data_ptr()
+        s.d_xnbr = self.nbr_d.data_ptr()
+        s.d_xwt = self.wt_d.data_ptr() if self.wt_d is not None else None
+
+
+class Op:
+    """y = (M0 + sum_S w b b^T + shift I) x  (realworld/polar_gpu.py:63-80)."""
+
+    def __init__(self, G):
+        self.G = G
+        self.M0 = G.M0
+        self.A = []
+        self.B = []
+        self._added = _Added(G)
+        self._scratch = {}
+
+    def add(self, a, b, w=1.0):
+        a, b = int(a), int(b)
+        if a == b or not (0 <= a < self.G.n and 0 <= b < self.G.n):
+            raise ValueError("added edge must join two distinct vertices")
+        self.A.append(a)
+        self.B.append(b)
+        self._added.add(a, b, float(w))
+
+    def struct(self):
+        return self.G.struct(self._added)
+
+    def __call__(self, x, shift=0.0):
+        """Apply to an (n, R) or (n,) float64/float32 CUDA tensor; returns a new tensor."""
+        squeeze = x.dim() == 1
+        X = x.reshape(self.G.n, -1)
+        if X.dtype not in (torch.float64, torch.float32):
+            raise TypeError("x must be float64 or float32")
+        if not X.is_cuda:
+            raise TypeError("x must be a CUDA tensor")
+        X = X.contiguous()
+        R = X.shape[1]
+        prec = _lib.POLAR_MIXED if X.dtype == torch.float32 else _lib.POLAR_FP64
+        maxc = 128 if prec == _lib.POLAR_MIXED else 64
+        Y = torch.empty_like(X)
+        g = self.struct()
+        lib = _lib.load()
+        stream = torch.cuda.current_stream(X.device).cuda_stream
+        key = (prec, X.device.index)
+        if key not in self._scratch:
+            nb = lib.polar_spmm_scratch_bytes(g, prec, maxc)
+            buf = torch.empty(max(nb, 256), dtype=torch.uint8, device=X.device)
+            _lib.check(lib.polar_spmm_scratch_init(g, prec, maxc, buf.data_ptr(), stream), "spmm scratch")
+            self._scratch[key] = buf
+        scratch = self._scratch[key]
+        for lo in range(0, R, maxc):
+            hi = min(R, lo + maxc)
+            xs = X[:, lo:hi]
+            ys = Y[:, lo:hi]
+            _lib.check(lib.polar_spmm(g, prec, hi - lo, float(shift), xs.data_ptr(), R, ys.data_ptr(), R,
+                                      scratch.data_ptr(), stream), "polar_spmm")
+        return Y.reshape(-1) if squeeze else Y

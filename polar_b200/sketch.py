@@ -1,0 +1,66 @@
+"""Sketch inputs Z (n x q), F = C_0^T U (n x q) and Gc (N x q), generated on the host.
+
+Same random stream and construction as realworld/polar_gpu.py:137-165 for the 'block'
+and 'gauss' kinds, so a seed reproduces the reference's sketches.  'rademacher' (entries
++-1/sqrt(q); Z centred) is an additional kind drawn in the same order (Z, then the
+edge-incidence rows U in 4M-edge chunks, then Gc).  Sketches are inputs of the timed
+path; the reference also builds them on the host, outside its timed region.
+"""
+import numpy as np
+import scipy.sparse as sp
+
+__all__ = ["sketches", "block_rows", "chunk_width"]
+
+
+def block_rows(rows, q, rng, center=False):
+    """Rows of independent Haar q x q orthogonal blocks (sign-fixed QR of Gaussians)."""
+    nb = -(-rows // q)
+    g = rng.normal(size=(nb, q, q))
+    Q, Rm = np.linalg.qr(g)
+    Q = Q * np.sign(np.diagonal(Rm, axis1=1, axis2=2))[:, None, :]
+    out = np.transpose(Q, (0, 2, 1)).reshape(nb * q, q)[:rows]
+    if center:
+        out = out - out.mean(0)
+    return out
+
+
+def _draw(kind, rows, q, rng, center=False):
+    if kind == "gauss":
+        out = rng.normal(size=(rows, q)) / np.sqrt(q)
+        return out
+    if kind == "rademacher":
+        out = (rng.integers(0, 2, size=(rows, q), dtype=np.int8) * 2 - 1).astype(np.float64) / np.sqrt(q)
+        if center:
+            out = out - out.mean(0)
+        return out
+    if kind == "block":
+        return block_rows(rows, q, rng, center=center)
+    raise ValueError(f"unknown sketch kind {kind!r}")
+
+
+def sketches(G, cand, q, seed, kind="block", chunk=4_000_000):
+    """(Z, F, Gc) as float64 host arrays."""
+    rng = np.random.default_rng(seed)
+    n = G.n
+    Z = _draw(kind, n, q, rng, center=(kind != "gauss"))
+    F = np.zeros((n, q))
+    u, v = G.edges[:, 0], G.edges[:, 1]
+    sw = np.sqrt(G.weights)
+    for lo in range(0, G.m, chunk):
+        hi = min(G.m, lo + chunk)
+        U = _draw(kind, hi - lo, q, rng)
+        U *= sw[lo:hi, None]
+        ne = hi - lo
+        C = sp.csr_matrix((np.r_[np.ones(ne), -np.ones(ne)],
+                           (np.r_[u[lo:hi], v[lo:hi]], np.r_[np.arange(ne), np.arange(ne)])), shape=(n, ne))
+        F += C @ U
+    Gc = _draw(kind, len(cand), q, rng)
+    return Z, F, Gc
+
+
+def chunk_width(n, p, nA, budget=10e9):
+    """The reference's bank width heuristic (realworld/polar_gpu.py:169-173), kept for the
+    API; the device path picks its own width from the kernel's column limit."""
+    per_col = 8.0 * (10 * n + 4 * p * nA)
+    cap = 16 if n > 3e6 else 64
+    return int(max(8, min(cap, budget // per_col)))

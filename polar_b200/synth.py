@@ -1,0 +1,123 @@
+"""Seeded synthetic inputs: Chung–Lu graphs and uniform non-edge candidate pools.
+
+The reference runs on SNAP graphs (realworld/graphs.py:11-19); those files are not
+available here, so seeded Chung–Lu graphs with the same vertex/edge counts stand in
+for them. Host-side NumPy: this is input generation, not part of the timed path.
+"""
+import numpy as np
+
+__all__ = ["chung_lu", "candidates", "CONFIGS", "make_config"]
+
+
+def _chung_lu_weights(n, mean_deg, gamma, dmax):
+    """Expected degrees w_i = C (i + i0)^(-1/(gamma-1)), sum w = n * mean_deg, w_0 = dmax.
+
+    i0 is found by bisection so that the largest expected degree equals `dmax`
+    (default: the structural cutoff sqrt(sum w), which keeps w_i w_j / sum w <= 1)."""
+    total = float(n) * float(mean_deg)
+    if dmax is None:
+        dmax = np.sqrt(total)
+    alpha = 1.0 / (gamma - 1.0)
+    i = np.arange(n, dtype=np.float64)
+
+    def top(i0):
+        base = (i + i0) ** (-alpha)
+        return total * base[0] / base.sum()
+
+    lo, hi = 1e-6, float(n)
+    if top(lo) < dmax:
+        i0 = lo
+    else:
+        for _ in range(200):
+            mid = np.sqrt(lo * hi)
+            if top(mid) > dmax:
+                lo = mid
+            else:
+                hi = mid
+        i0 = hi
+    w = (i + i0) ** (-alpha)
+    return w * (total / w.sum())
+
+
+def chung_lu(n, mean_deg, gamma, seed, dmax=None, m=None):
+    """Undirected simple Chung–Lu graph on vertices 0..n-1 (hubs at low ids).
+
+    Endpoints are drawn independently with probability proportional to the expected
+    degree; the result is made undirected, stripped of self-loops and deduplicated with
+    the same preprocessing rule as realworld/graphs.py:52-53 (sort each pair, drop u==v,
+    unique).  Sampling repeats until exactly `m` distinct edges exist (default
+    round(n*mean_deg/2)); a final seeded subset trims any overshoot.
+    Returns int64[m, 2] with u < v, rows sorted lexicographically."""
+    rng = np.random.default_rng(seed)
+    w = _chung_lu_weights(n, mean_deg, gamma, dmax)
+    target = int(round(n * mean_deg / 2)) if m is None else int(m)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    keys = np.empty(0, dtype=np.int64)
+    while len(keys) < target:
+        need = target - len(keys)
+        draw = int(need * 1.15) + 64
+        u = np.searchsorted(cdf, rng.random(draw), side="right").clip(0, n - 1)
+        v = np.searchsorted(cdf, rng.random(draw), side="right").clip(0, n - 1)
+        a = np.minimum(u, v).astype(np.int64)
+        b = np.maximum(u, v).astype(np.int64)
+        keep = a != b
+        keys = np.unique(np.concatenate([keys, a[keep] * n + b[keep]]))
+    if len(keys) > target:
+        keys = keys[np.sort(rng.choice(len(keys), target, replace=False))]
+    return np.stack([keys // n, keys % n], axis=1).astype(np.int64)
+
+
+def candidates(n, edges, N, seed):
+    """Uniform random non-edge pool, the rule of realworld/graphs.py:61-69.
+
+    Pairs (u, v) with u < v are drawn one at a time with `rng.integers(n, size=2)`,
+    rejected when u == v or when the pair is an edge, and collected until N distinct
+    pairs exist; the pool is then sorted and shuffled with `rng.permutation(N)`.  Drawing
+    one pair per call keeps the random stream identical to the reference rule, so the
+    same seed yields the same pool."""
+    keys = np.sort(edges[:, 0].astype(np.int64) * n + edges[:, 1].astype(np.int64))
+    rng = np.random.default_rng(seed)
+    chosen = set()
+    integers = rng.integers
+    search = np.searchsorted
+    nk = len(keys)
+    while len(chosen) < N:
+        x, y = integers(n, size=2)
+        u, v = (int(x), int(y)) if x <= y else (int(y), int(x))
+        if u == v:
+            continue
+        key = u * n + v
+        i = search(keys, key)
+        if i < nk and keys[i] == key:
+            continue
+        chosen.add((u, v))
+    c = np.asarray(sorted(chosen), dtype=np.int64)
+    return np.ascontiguousarray(c[rng.permutation(N)])
+
+
+# Workload shapes.  Each entry: graph (n, mean degree, exponent, seed, dmax), pool size N,
+# pole count K, sketch width q, shortlist B, rounds k, sigma, s, CG tolerance.
+CONFIGS = {
+    "plain-n2000": dict(n=2000, mean_deg=6.0, gamma=2.5, seed=0, dmax=None, N=20000,
+                        K=16, q=32, B=1, k=10, sigma=1e-2, s=0.5, tol=1e-8),
+    "precision-n317k": dict(n=317080, mean_deg=2 * 1049866 / 317080, gamma=2.4, seed=1, dmax=None,
+                            N=200000, K=24, q=64, B=16, k=50, sigma=1e-2, s=0.5, tol=1e-7),
+    "diff-n1.13M": dict(n=1134890, mean_deg=2 * 2987624 / 1134890, gamma=2.2, seed=3, dmax=None,
+                        N=4096, K=24, q=64, B=16, k=0, sigma=1e-2, s=0.5, tol=1e-7),
+    "full-n4M": dict(n=3997962, mean_deg=2 * 34681189 / 3997962, gamma=2.1, seed=4, dmax=15000,
+                     N=1000000, K=32, q=64, B=16, k=100, sigma=1e-2, s=0.5, tol=1e-6),
+}
+
+
+def make_config(name, n=None, N=None, cand_seed=None):
+    """Build (edges, n, cand) for a named workload, optionally shrunk to `n` vertices
+    (mean degree and exponent kept) and `N` candidates."""
+    c = dict(CONFIGS[name])
+    n = c["n"] if n is None else int(n)
+    N = c["N"] if N is None else int(N)
+    dmax = c["dmax"] if n == c["n"] else None
+    edges = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=dmax)
+    seed = c["seed"] + 7919 if cand_seed is None else cand_seed
+    cand = candidates(n, edges, N, seed)
+    return edges, n, cand, c

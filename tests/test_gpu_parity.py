@@ -1,0 +1,234 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with golden vectors of
+the unmodified reference.  Needs a B200."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import polar_oracle as O
+from polar_b200.synth import chung_lu, candidates
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD / "reference_vectors.npz"), json.loads((GOLD / "reference_vectors.json").read_text())
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+# ---------------------------------------------------------------------------------------
+# SpMM (realworld/spmm.py, polar_gpu.py:71-80)
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("R", [1, 3, 16, 64, 128])
+@pytest.mark.parametrize("heavy", [256, 8])
+def test_spmm_matches_scipy(torch_cuda, prec, R, heavy):
+    import polar_b200 as pg
+    torch = torch_cuda
+    n = 4000
+    E = chung_lu(n, 6.0, 2.2, 9)
+    G = pg.Graph(n, E, 1e-2, heavy_thresh=heavy)
+    op = pg.Op(G)
+    ref = O.Op(O.Graph(n, E, 1e-2))
+    for a, b in [(0, 5), (17, 3999), (0, 17)]:
+        op.add(a, b)
+        ref.add(a, b)
+    rng = np.random.default_rng(R)
+    X = rng.normal(size=(n, R))
+    dt = torch.float64 if prec == "fp64" else torch.float32
+    Y = op(torch.as_tensor(X, dtype=dt, device="cuda"), 0.37).double().cpu().numpy()
+    Yr = ref(X, 0.37)
+    tol = 1e-13 if prec == "fp64" else 2e-6
+    assert _rel(Y, Yr) < tol
+
+
+def test_spmm_weighted(torch_cuda):
+    import polar_b200 as pg
+    torch = torch_cuda
+    z = np.load(GOLD / "reference_vectors.npz")
+    E, w = z["g1_edges"], z["g1w_weights"]
+    G = pg.Graph(300, E, 0.1, weights=w, heavy_thresh=4)
+    op = pg.Op(G)
+    ref = O.Op(O.Graph(300, E, 0.1, weights=w))
+    op.add(1, 2, 0.5)
+    X = np.random.default_rng(0).normal(size=(300, 8))
+    Y = op(torch.as_tensor(X, device="cuda"), 0.0).cpu().numpy()
+    Yr = ref.M0 @ X
+    d = 0.5 * (X[1] - X[2])
+    Yr[1] += d
+    Yr[2] -= d
+    assert _rel(Y, Yr) < 1e-13
+
+
+# ---------------------------------------------------------------------------------------
+# msolve (polar_gpu.py:88-133)
+def _ms_inputs(gold, pg):
+    z, meta = gold
+    G = pg.Graph(300, z["g1_edges"], 1e-2)
+    op = pg.Op(G)
+    for a, b in meta["ms_added"]:
+        op.add(a, b)
+    return z, op
+
+
+def test_msolve_fp64_matches_reference(gold, torch_cuda):
+    import polar_b200 as pg
+    z, op = _ms_inputs(gold, pg)
+    X, h, it = pg.msolve(op, z["ms_W"], z["ms_tau"], z["ms_active"], 1e-10, track=True)
+    X = X.cpu().numpy()
+    assert _rel(X, z["ms_X"]) < 1e-8
+    assert _rel(h.cpu().numpy(), z["ms_h"]) < 1e-8
+    assert np.max(np.abs(it - z["ms_iters"])) <= 2
+    assert it[3] == 0 and np.all(X[:, :, 3] == 0)
+
+
+def test_msolve_mixed_close_to_reference(gold, torch_cuda):
+    import polar_b200 as pg
+    z, op = _ms_inputs(gold, pg)
+    X, h, it = pg.msolve(op, z["ms_W"], z["ms_tau"], z["ms_active"], 1e-7, track=True, precision="mixed")
+    assert X.dtype.is_floating_point and X.element_size() == 4
+    assert _rel(X.cpu().numpy(), z["ms_X"]) < 1e-4
+    assert _rel(h.cpu().numpy(), z["ms_h"]) < 1e-5
+
+
+def test_msolve_heavy_split_and_determinism(torch_cuda):
+    import polar_b200 as pg
+    torch = torch_cuda
+    n = 3000
+    E = chung_lu(n, 6.0, 2.1, 4)
+    tau, om, _ = pg.poles("frac", 0.5, 1e-2, 500.0, 1e-2, K=12)
+    W = np.random.default_rng(1).normal(size=(n, 8))
+    active = np.arange(0, n, 3)
+    outs = []
+    for thresh in (100000, 7, 7):
+        G = pg.Graph(n, E, 1e-2, heavy_thresh=thresh)
+        X, h, it = pg.msolve(pg.Op(G), W, tau, active, 1e-9, track=True)
+        outs.append((X.cpu().numpy(), h.cpu().numpy(), it))
+    assert _rel(outs[1][0], outs[0][0]) < 1e-8
+    assert np.array_equal(outs[1][0], outs[2][0]) and np.array_equal(outs[1][1], outs[2][1])
+    Xo, ho, ito = O.msolve(O.Op(O.Graph(n, E, 1e-2)), W, tau, active, 1e-9, track=True)
+    assert _rel(outs[1][0], Xo) < 1e-8 and _rel(outs[1][1], ho) < 1e-8
+    assert np.max(np.abs(outs[1][2] - ito)) <= 2
+
+
+def test_msolve_errors(torch_cuda):
+    import polar_b200 as pg
+    from polar_b200 import _lib
+    z = np.load(GOLD / "reference_vectors.npz")
+    G = pg.Graph(300, z["g1_edges"], 1e-2)
+    op = pg.Op(G)
+    tau = z["ms_tau"]
+    W = z["ms_W"]
+    with pytest.raises(RuntimeError, match="iteration cap"):
+        pg.msolve(op, W, tau, z["ms_active"], 1e-12, maxit=5)
+    Wn = W.copy()
+    Wn[3, 1] = np.nan
+    with pytest.raises(_lib.PolarError) as ei:
+        pg.msolve(op, Wn, tau, z["ms_active"], 1e-10)
+    assert ei.value.status == _lib.POLAR_ERR_NONFINITE
+    # a barrier wait that runs out returns TIMEOUT and leaves the context usable
+    lib = _lib.load()
+    lib.polar_set_barrier_timeout_ns(1)
+    try:
+        with pytest.raises(_lib.PolarError) as ei:
+            pg.msolve(op, W, tau, z["ms_active"], 1e-10)
+        assert ei.value.status == _lib.POLAR_ERR_TIMEOUT
+    finally:
+        lib.polar_set_barrier_timeout_ns(4_000_000_000)
+    X, h, it = pg.msolve(op, W, tau, z["ms_active"], 1e-10, track=True)
+    assert np.isfinite(X.cpu().numpy()).all()
+
+
+# ---------------------------------------------------------------------------------------
+# greedy (polar_gpu.py:180-254) against the reference's own sequences
+RUNS = ["frac_B4_K12", "frac_B1_K12", "frac_s025_B3_K10", "er_B4", "logdet_B4", "naive_K12", "frac_B2_eps"]
+
+
+@pytest.fixture(scope="module")
+def g2(gold, torch_cuda):
+    import polar_b200 as pg
+    z, _ = gold
+    G = pg.Graph(500, z["g2_edges"], 1e-2)
+    cand = z["g2_cand"]
+    sk = pg.sketches(G, cand, 16, 2026)
+    return G, cand, sk
+
+
+@pytest.mark.parametrize("name", RUNS)
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_polar_sequence_matches_reference(gold, g2, name, prec):
+    import polar_b200 as pg
+    z, meta = gold
+    cfg = meta["runs"][name]
+    G, cand, sk = g2
+    trace = []
+    res = pg.polar(G, cand, cfg["k"], cfg["s"], q=16, B=cfg["B"], eps=cfg.get("eps", 1e-2), tol=1e-8,
+                   obj=cfg["obj"], sketch=sk, naive=cfg.get("naive", False), trace=trace, K=cfg["K"],
+                   precision=prec)
+    assert res["sequence"] == list(z[f"run_{name}_sequence"])
+    assert res["p"] == int(z[f"run_{name}_p"])
+    key = f"run_{name}_rerank_max"
+    if key in z.files:
+        tol = 1e-9 if prec == "fp64" else 1e-6
+        np.testing.assert_allclose(res["marginals"], z[key], rtol=tol)
+    if prec == "fp64":
+        np.testing.assert_array_equal(np.array([t["shortlist"] for t in trace]), z[f"run_{name}_shortlists"])
+        assert abs(res["spmv"] - int(z[f"run_{name}_spmv"])) <= 2 * cfg["k"] + 2
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_plain_workload_matches_reference(gold, torch_cuda, prec):
+    import polar_b200 as pg
+    z, _ = gold
+    E = chung_lu(2000, 6.0, 2.5, 0)
+    cand = candidates(2000, E, 20000, 7919)
+    G = pg.Graph(2000, E, 1e-2)
+    sk = pg.sketches(G, cand, 32, 2026)
+    res = pg.polar(G, cand, 10, 0.5, q=32, B=1, tol=1e-8, sketch=sk, K=16, precision=prec)
+    assert res["sequence"] == list(z["plain_sequence"])
+    ores = O.polar(O.Graph(2000, E, 1e-2), cand, 10, 0.5, q=32, B=1, tol=1e-8, sketch=sk, K=16)
+    tol = 1e-9 if prec == "fp64" else 1e-6
+    np.testing.assert_allclose(res["marginals"], ores["marginals"], rtol=tol)
+
+
+def test_true_marginals_match_reference(gold, g2):
+    import polar_b200 as pg
+    z, meta = gold
+    G, cand, _ = g2
+    for obj in ("frac", "er", "logdet"):
+        g, cert = pg.true_marginals(G, cand, meta["tm_seq"], 0.5, obj=obj, eps=1e-4, tol=1e-10)
+        np.testing.assert_allclose(g, z[f"tm_{obj}"], rtol=1e-9)
+        assert cert["residual_rho"] == pytest.approx(float(z[f"tm_{obj}_rho"]))
+
+
+def test_true_marginals_match_dense_eigs(g2):
+    """Certified marginals vs a dense FP64 eigendecomposition (realworld/validate.py:26-43)."""
+    import polar_b200 as pg
+    G, cand, _ = g2
+    seq = [3, 17, 101, 250]
+    g, cert = pg.true_marginals(G, cand, seq, 0.5, obj="frac", eps=1e-9, tol=1e-11)
+    M = G.M0.get().toarray()
+    prev = np.sum(np.linalg.eigvalsh(M) ** -0.5)
+    for e, ge in zip(seq, g):
+        a, b = cand[e]
+        M[a, a] += 1
+        M[b, b] += 1
+        M[a, b] -= 1
+        M[b, a] -= 1
+        cur = np.sum(np.linalg.eigvalsh(M) ** -0.5)
+        assert abs((prev - cur) - ge) / (prev - cur) < 1e-7
+        prev = cur

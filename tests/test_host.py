@@ -1,0 +1,135 @@
+"""Host-side logic and the C-ABI library surface.  CPU only."""
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import polar_b200 as pg
+from oracle import polar_oracle as O
+from polar_b200 import _lib
+from polar_b200.synth import chung_lu
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLD = ROOT / "tests" / "golden"
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / "include" / "polar.h").read_text()
+    declared = set(re.findall(r"^\s*(?:[\w\*\s]+?)\b(polar_\w+)\s*\(", header, re.M))
+    assert len(declared) >= 18
+    lib = _lib.load()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(_lib.SIGNATURES) == declared
+    assert lib.polar_version() >= 1
+
+
+def test_quadrature_matches_oracle_and_reference():
+    z = np.load(GOLD / "reference_vectors.npz")
+    import json
+    meta = json.loads((GOLD / "reference_vectors.json").read_text())
+    for i, (s, a, zz, eps) in enumerate(meta["composite_cases"]):
+        tau, om, b = pg.composite(s, a, zz, eps)
+        np.testing.assert_allclose(tau, z[f"composite{i}_tau"], rtol=1e-13)
+        np.testing.assert_allclose(om, z[f"composite{i}_om"], rtol=1e-12)
+    for s in (0.25, 0.5, 0.75):
+        for K in (8, 16, 24, 32):
+            t1, o1 = pg.fixed_rule(s, K, 3.0)
+            t2, o2 = O.fixed_rule(s, K, 3.0)
+            np.testing.assert_allclose(t1, t2, rtol=1e-13)
+            np.testing.assert_allclose(o1, o2, rtol=1e-13)
+            assert np.all(np.diff(t1) > 0) and np.all(o1 > 0)
+
+
+@pytest.mark.parametrize("s", [0.25, 0.5, 0.75])
+def test_fixed_rule_reproduces_power(s):
+    # sum_j om_j / (x + tau_j) ~= x^-s on [sigma, Lam]; the error falls with K.
+    sigma, Lam = 1e-2, 300.0
+    x = np.geomspace(sigma, Lam, 200)
+    errs = []
+    for K in (8, 16, 32):
+        tau, om = pg.fixed_rule(s, K, np.sqrt(sigma * Lam))
+        approx = (om[None, :] / (x[:, None] + tau[None, :])).sum(1)
+        errs.append(np.max(np.abs(approx / x ** (-s) - 1)))
+    assert errs[0] > errs[1] > errs[2]
+    assert errs[2] < 2e-4  # K=32 on a 3e4 spectral range
+
+
+def test_composite_rule_known_answer():
+    # Quadrature KAT of synthetic/controls/verify_stieltjes.py:43-52: on a dense n=50
+    # graph the composite-rule marginals match eigenvalue marginals within 256*4^-r.
+    rng = np.random.default_rng(7)
+    n, sigma, s = 50, 0.5, 0.5
+    A = np.triu(rng.random((n, n)) < 0.08, 1)
+    A = (A + A.T).astype(float)
+    i = np.arange(n)
+    A[i, (i + 1) % n] = A[(i + 1) % n, i] = 1.0
+    M = np.diag(A.sum(1)) - A + sigma * np.eye(n)
+    lam = np.linalg.eigvalsh(M)
+    pairs = np.argwhere(np.triu(A == 0, 1))[:200]
+    E = np.zeros((n, len(pairs)))
+    E[pairs[:, 0], np.arange(len(pairs))] = 1
+    E[pairs[:, 1], np.arange(len(pairs))] = -1
+    exact = np.array([np.sum(lam ** -s) - np.sum(np.linalg.eigvalsh(M + np.outer(b, b)) ** -s) for b in E.T])
+    for eps in (1e-1, 1e-2, 1e-4):
+        tau, om, bound = pg.composite(s, sigma, lam[-1] + 2, eps)
+        approx = np.zeros(len(pairs))
+        for tj, wj in zip(tau, om):
+            X = np.linalg.solve(M + tj * np.eye(n), E)
+            approx += wj * np.sum(X * X, 0) / (1 + np.sum(E * X, 0))
+        assert np.max(np.abs(approx - exact) / exact) <= bound
+
+
+def test_sketches_match_reference():
+    z = np.load(GOLD / "reference_vectors.npz")
+    G = O.Graph(300, z["g1_edges"], 1e-2)
+    cand = z["g1_cand"]
+    for kind in ("block", "gauss"):
+        Z, F, Gc = pg.sketches(G, cand, 8, 2026, kind=kind)
+        np.testing.assert_allclose(Z, z[f"g1_sk_{kind}_Z"], rtol=0, atol=1e-14)
+        np.testing.assert_allclose(F, z[f"g1_sk_{kind}_F"], rtol=0, atol=1e-14)
+        np.testing.assert_allclose(Gc, z[f"g1_sk_{kind}_Gc"], rtol=0, atol=1e-14)
+    Z, F, Gc = pg.sketches(G, cand, 16, 5, kind="rademacher")
+    assert np.allclose(np.abs(Gc), 0.25) and np.allclose(Z.mean(0), 0)
+    assert np.allclose(np.linalg.norm(Gc, axis=1), 1.0)
+
+
+def test_chung_lu_shape():
+    E = chung_lu(5000, 8.0, 2.2, 3, dmax=400)
+    assert len(E) == 20000
+    assert np.all(E[:, 0] < E[:, 1])
+    assert len(np.unique(E[:, 0] * 5000 + E[:, 1])) == len(E)
+    deg = np.bincount(E.ravel(), minlength=5000)
+    assert 150 < deg.max() <= 800
+
+
+def test_graph_host_structures_and_heavy_split():
+    import torch
+    E = chung_lu(3000, 6.0, 2.2, 5)
+    G = pg.Graph(3000, E, 1e-2, heavy_thresh=16, device="cpu")
+    M = O.Graph(3000, E, 1e-2).M0
+    assert (G.M0.get() != M).nnz == 0
+    degs = np.diff(G._indptr_h)
+    heavy = np.flatnonzero(degs > 16)
+    assert G.nheavy == len(heavy) > 0
+    lo = G.chunk_lo.numpy()
+    hi = G.chunk_hi.numpy()
+    row = G.chunk_row.numpy()
+    off = G.hchunk_off.numpy()
+    for h, r in enumerate(heavy):
+        segs = list(zip(lo[off[h]:off[h + 1]], hi[off[h]:off[h + 1]]))
+        assert segs[0][0] == G._indptr_h[r] and segs[-1][1] == G._indptr_h[r + 1]
+        assert all(b0 == a1 for (_, a1), (b0, _) in zip(segs[:-1], segs[1:]))
+        assert all(b - a <= 16 for a, b in segs)
+        assert np.all(row[off[h]:off[h + 1]] == h)
+    s = G.struct()
+    assert s.nheavy == G.nheavy and s.nchunks == G.nchunks and s.d_wts is None
+    assert G.Lam(3) == pytest.approx(1e-2 + 2 * G.dmax + 12)
+
+
+def test_status_mapping():
+    with pytest.raises(RuntimeError, match="iteration cap"):
+        _lib.check(_lib.POLAR_ERR_ITER_CAP)
+    with pytest.raises(_lib.PolarError):
+        _lib.check(_lib.POLAR_ERR_BAD_ARG, "x")
