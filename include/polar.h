@@ -90,6 +90,10 @@ typedef struct polar_msolve_info {
   int64_t flushes;       /* deferred shifted-update passes */
   int32_t error_where;   /* phase code where a barrier wait timed out (0 = none) */
   int32_t pad;
+  /* wall time per phase seen by CTA 0, barriers included (ns): [0] deferred shifted
+   * updates, [1] SpMM + d.v reduction, [2] residual update + r.r reduction,
+   * [3] pole recurrences + direction update, [4] final pass, [5] initialisation */
+  int64_t phase_ns[6];
 } polar_msolve_info;
 
 /* ---- error text of the last failing call on this host thread ---- */

@@ -52,7 +52,7 @@ class PolarGraph(ctypes.Structure):
 class MsolveInfo(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int32), ("ld", ctypes.c_int32), ("grid", ctypes.c_int32),
                 ("block", ctypes.c_int32), ("iterations", ctypes.c_int64), ("flushes", ctypes.c_int64),
-                ("error_where", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("error_where", ctypes.c_int32), ("pad", ctypes.c_int32), ("phase_ns", ctypes.c_int64 * 6)]
 
 
 _P = ctypes.c_void_p

@@ -40,9 +40,11 @@ POLAR_D RowGroup make_row_group(int ld) {
 }
 
 // acc[v] += sum_{k in [lo,hi)} w_k * X[idx_k][col+v]
+// Lanes with on == false (all their columns converged) still take part in the index
+// shuffles but issue no loads.
 template <typename T, int VEC, bool WEIGHTED>
 POLAR_D void gather_rows(const polar_graph& g, const RowGroup& rg, int lo, int hi, const T* X,
-                         int ld, typename AccOf<T>::type (&acc)[VEC]) {
+                         int ld, typename AccOf<T>::type (&acc)[VEC], bool on = true) {
   using A = typename AccOf<T>::type;
   for (int k0 = lo; k0 < hi; k0 += rg.G) {
     const int k = k0 + rg.lg;
@@ -62,21 +64,25 @@ POLAR_D void gather_rows(const polar_graph& g, const RowGroup& rg, int lo, int h
         jj[u] = __shfl_sync(rg.mask, j, t + u, rg.G);
         ww[u] = WEIGHTED ? __shfl_sync(rg.mask, w, t + u, rg.G) : A(1);
       }
-      T xv[4][VEC];
+      if (on) {
+        T xv[4][VEC];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) vload<T, VEC>(xv[u], X + (size_t)jj[u] * ld + rg.col);
+        for (int u = 0; u < 4; ++u) vload<T, VEC>(xv[u], X + (size_t)jj[u] * ld + rg.col);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < VEC; ++v) acc[v] = WEIGHTED ? fma(ww[u], (A)xv[u][v], acc[v]) : acc[v] + (A)xv[u][v];
+          for (int v = 0; v < VEC; ++v) acc[v] = WEIGHTED ? fma(ww[u], (A)xv[u][v], acc[v]) : acc[v] + (A)xv[u][v];
+      }
     }
     for (; t < cnt; ++t) {
       const int jj = __shfl_sync(rg.mask, j, t, rg.G);
       const A ww = WEIGHTED ? __shfl_sync(rg.mask, w, t, rg.G) : A(1);
-      T xv[VEC];
-      vload<T, VEC>(xv, X + (size_t)jj * ld + rg.col);
+      if (on) {
+        T xv[VEC];
+        vload<T, VEC>(xv, X + (size_t)jj * ld + rg.col);
 #pragma unroll
-      for (int v = 0; v < VEC; ++v) acc[v] = WEIGHTED ? fma(ww, (A)xv[v], acc[v]) : acc[v] + (A)xv[v];
+        for (int v = 0; v < VEC; ++v) acc[v] = WEIGHTED ? fma(ww, (A)xv[v], acc[v]) : acc[v] + (A)xv[v];
+      }
     }
   }
 }
@@ -84,9 +90,9 @@ POLAR_D void gather_rows(const polar_graph& g, const RowGroup& rg, int lo, int h
 // Added-edge contribution for row i: acc += sum w x_k, returns sum w (to add to diag).
 template <typename T, int VEC>
 POLAR_D double added_terms(const polar_graph& g, const RowGroup& rg, int i, const T* X, int ld,
-                           typename AccOf<T>::type (&acc)[VEC]) {
+                           typename AccOf<T>::type (&acc)[VEC], bool on = true) {
   using A = typename AccOf<T>::type;
-  if (g.nx == 0) return 0.0;
+  if (g.nx == 0 || !on) return 0.0;
   const uint32_t bits = __ldg(g.d_xbits + (i >> 5));
   if (!((bits >> (i & 31)) & 1u)) return 0.0;
   int lo = 0, hi = g.nx - 1;
@@ -114,6 +120,11 @@ POLAR_D void finish_row(const polar_graph& g, const RowGroup& rg, int i, int deg
                         const T* X, int ld, typename AccOf<T>::type (&acc)[VEC], T* Y,
                         int ldy, T (&xi)[VEC], T (&yi)[VEC], bool store = true) {
   using A = typename AccOf<T>::type;
+  if (!store) {  // lane idle: nothing to compute
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) xi[v] = yi[v] = T(0);
+    return;
+  }
   const double wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
   vload<T, VEC>(xi, X + (size_t)i * ld + rg.col);

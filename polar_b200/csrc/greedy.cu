@@ -60,8 +60,8 @@ POLAR_D bool better(double s1, long long i1, double s2, long long i2) {
   return s1 > s2 || (s1 == s2 && i1 < i2);
 }
 
-constexpr int kTopBlock = 512;
-constexpr int kTopPer = 8;  // elements per thread in the scoring pass
+constexpr int kTopBlock = 256;
+constexpr int kTopPer = 2;  // elements per thread in the scoring and merge passes
 constexpr int kMaxB = 64;
 
 struct Cand {
@@ -142,6 +142,36 @@ __global__ void __launch_bounds__(kTopBlock) score_block_topb_kernel(const doubl
   }
 }
 
+// One level of the candidate merge: each CTA keeps the B best of its 512 candidates.
+__global__ void __launch_bounds__(kTopBlock) topb_level_kernel(const Cand* in, int n_in, int B, Cand* out) {
+  __shared__ Cand sh[33];
+  double s[kTopPer];
+  long long idx[kTopPer];
+#pragma unroll
+  for (int k = 0; k < kTopPer; ++k) {
+    const long long e = (long long)blockIdx.x * kTopBlock * kTopPer + (long long)k * kTopBlock + threadIdx.x;
+    if (e < n_in) {
+      const Cand c = in[e];
+      s[k] = c.s;
+      idx[k] = c.i;
+    } else {
+      s[k] = -INFINITY;
+      idx[k] = LLONG_MAX;
+    }
+  }
+  for (int b = 0; b < B; ++b) {
+    Cand mine{-INFINITY, LLONG_MAX};
+#pragma unroll
+    for (int k = 0; k < kTopPer; ++k)
+      if (idx[k] != LLONG_MAX && better(s[k], idx[k], mine.s, mine.i)) mine = Cand{s[k], idx[k]};
+    const Cand w = block_best(mine, sh);
+    if (threadIdx.x == 0) out[(size_t)blockIdx.x * B + b] = w;
+#pragma unroll
+    for (int k = 0; k < kTopPer; ++k)
+      if (idx[k] == w.i) idx[k] = LLONG_MAX;
+  }
+}
+
 __global__ void __launch_bounds__(1024) merge_topb_kernel(const Cand* blk, int ncand, int B, int64_t* out_idx,
                                                           double* out_score) {
   __shared__ Cand sh[33];
@@ -202,7 +232,7 @@ __global__ void rerank_kernel(const void* U, int u_f32, int p, int nA, int ldu, 
 // ---------------------------------------------------------------------------------------
 // Maintenance (polar_gpu.py:242-249).
 struct MaintTmp {
-  double *xi, *eta, *D, *nxi, *neta, *wX, *wY;
+  double *xi, *eta, *D, *nxi, *neta, *wX, *wY, *xiD, *etaD;
 };
 
 POLAR_HD size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -218,11 +248,13 @@ static MaintTmp maint_tmp(void* base, int p, int nA, int q) {
   m.neta = (double*)(b + o); o += al256((size_t)p * 8);
   m.wX = (double*)(b + o); o += al256((size_t)p * nA * 8);
   m.wY = (double*)(b + o); o += al256((size_t)p * nA * 8);
+  m.xiD = (double*)(b + o); o += al256((size_t)p * q * 8);
+  m.etaD = (double*)(b + o); o += al256((size_t)p * q * 8);
   return m;
 }
 
 static size_t maint_tmp_bytes(int p, int nA, int q) {
-  return al256((size_t)p * q * 8) * 2 + al256((size_t)p * 8) * 3 + al256((size_t)p * nA * 8) * 2;
+  return al256((size_t)p * q * 8) * 4 + al256((size_t)p * 8) * 3 + al256((size_t)p * nA * 8) * 2;
 }
 
 // one CTA per pole
@@ -254,12 +286,20 @@ __global__ void maint_setup_kernel(const void* X, int ldx, const void* Y, int ld
     }
     m.nxi[j] = t1;
     m.neta[j] = t2;
-    m.D[j] = 1.0 + ldv(U, u_f32, ((size_t)j * nA + a) * ldu + uc) - ldv(U, u_f32, ((size_t)j * nA + b) * ldu + uc);
+    s1[0] = 1.0 + ldv(U, u_f32, ((size_t)j * nA + a) * ldu + uc) - ldv(U, u_f32, ((size_t)j * nA + b) * ldu + uc);
+    m.D[j] = s1[0];
+  }
+  __syncthreads();
+  const double D = s1[0];
+  for (int c = threadIdx.x; c < q; c += blockDim.x) {
+    m.xiD[(size_t)j * q + c] = m.xi[(size_t)j * q + c] / D;
+    m.etaD[(size_t)j * q + c] = m.eta[(size_t)j * q + c] / D;
   }
 }
 
-// One 16-lane group per (pole, active row): w = row . dir, then row -= / += u dir / D.
-template <typename T>
+// One 16-lane group per (pole, active row): w = row . dir (before the update), then
+// X_row -= u xi/D, Y_row += u eta/D.  Lanes own VEC consecutive columns (vector loads).
+template <typename T, int VEC>
 __global__ void maint_rows_kernel(T* X, int ldx, T* Y, int ldy, int p, int nA, int q, const void* U, int u_f32,
                                   int ldu, const int32_t* win, MaintTmp m) {
   const int lanes = 16;
@@ -270,18 +310,27 @@ __global__ void maint_rows_kernel(T* X, int ldx, T* Y, int ldy, int p, int nA, i
   const int j = (int)(gidx / nA), a = (int)(gidx % nA);
   const int uc = win[0];
   const double u = ldv(U, u_f32, ((size_t)j * nA + a) * ldu + uc);
-  const double D = m.D[j];
   T* xr = X + ((size_t)j * nA + a) * ldx;
   T* yr = Y + ((size_t)j * nA + a) * ldy;
   const double* xi = m.xi + (size_t)j * q;
   const double* eta = m.eta + (size_t)j * q;
+  const double* xiD = m.xiD + (size_t)j * q;
+  const double* etaD = m.etaD + (size_t)j * q;
   double wx = 0.0, wy = 0.0;
-  for (int c = lg; c < q; c += lanes) {
-    const double xv = (double)xr[c], yv = (double)yr[c];
-    wx += xv * xi[c];
-    wy += yv * eta[c];
-    xr[c] = (T)(xv - u * xi[c] / D);
-    yr[c] = (T)(yv + u * eta[c] / D);
+  for (int c = lg * VEC; c < q; c += lanes * VEC) {
+    T xv[VEC], yv[VEC];
+    vload<T, VEC>(xv, xr + c);
+    vload<T, VEC>(yv, yr + c);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const double x = (double)xv[v], y = (double)yv[v];
+      wx = fma(x, __ldg(xi + c + v), wx);
+      wy = fma(y, __ldg(eta + c + v), wy);
+      xv[v] = (T)fma(-u, __ldg(xiD + c + v), x);
+      yv[v] = (T)fma(u, __ldg(etaD + c + v), y);
+    }
+    vstore<T, VEC>(xr + c, xv);
+    vstore<T, VEC>(yr + c, yv);
   }
   for (int o = 8; o > 0; o >>= 1) {
     wx += __shfl_xor_sync(mask, wx, o);
@@ -376,7 +425,7 @@ extern "C" int polar_pair_norms(const void* d_X, int x_f32, int p, int nA, int l
 extern "C" size_t polar_topb_tmp_bytes(int N, int B) {
   const long long per = (long long)kTopBlock * kTopPer;
   const long long nb = (N + per - 1) / per;
-  return (size_t)(nb > 0 ? nb : 1) * (B > 0 ? B : 1) * sizeof(Cand);
+  return 2 * (size_t)(nb > 0 ? nb : 1) * (B > 0 ? B : 1) * sizeof(Cand) + 256;
 }
 
 extern "C" int polar_score_topb(const double* d_h, const double* d_t, const double* d_tau, const double* d_om,
@@ -393,12 +442,25 @@ extern "C" int polar_score_topb(const double* d_h, const double* d_t, const doub
                                                     (Cand*)d_tmp);
   int rc = check_launch("score_block_topb");
   if (rc) return rc;
-  const int ncand = nb * B;
+  // merge levels until one CTA can take the rest
+  const long long per_lvl = (long long)kTopBlock * kTopPer;
+  Cand* a = (Cand*)d_tmp;
+  Cand* b2 = a + (size_t)nb * B;
+  long long ncand = (long long)nb * B;
+  while (ncand > 4096) {
+    const int nb2 = (int)((ncand + per_lvl - 1) / per_lvl);
+    topb_level_kernel<<<nb2, kTopBlock, 0, st>>>(a, (int)ncand, B, b2);
+    rc = check_launch("topb_level");
+    if (rc) return rc;
+    Cand* t = a;
+    a = b2;
+    b2 = t;
+    ncand = (long long)nb2 * B;
+  }
   const size_t smem = (size_t)ncand * sizeof(Cand);
-  if (smem > 200 * 1024) return set_error(POLAR_ERR_UNSUPPORTED, "too many top-B candidates");
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(merge_topb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  merge_topb_kernel<<<1, 1024, smem, st>>>((const Cand*)d_tmp, ncand, B, d_out_idx, d_out_score);
+  merge_topb_kernel<<<1, 1024, smem, st>>>(a, (int)ncand, B, d_out_idx, d_out_score);
   return check_launch("merge_topb");
 }
 
@@ -438,12 +500,22 @@ extern "C" int polar_maintain(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32
   if (rc) return rc;
   const long long thr = (long long)p * nA * 16;
   const int blocks = (int)((thr + 255) / 256);
-  if (xy_f32)
-    maint_rows_kernel<float><<<blocks, 256, 0, st>>>((float*)d_X, ldx, (float*)d_Y, ldy, p, nA, q, d_U, u_f32, ldu,
-                                                     d_win, m);
-  else
-    maint_rows_kernel<double><<<blocks, 256, 0, st>>>((double*)d_X, ldx, (double*)d_Y, ldy, p, nA, q, d_U, u_f32, ldu,
-                                                      d_win, m);
+  const uintptr_t al = (uintptr_t)d_X | (uintptr_t)d_Y;
+  if (xy_f32) {
+    if (q % 4 == 0 && ldx % 4 == 0 && ldy % 4 == 0 && al % 16 == 0)
+      maint_rows_kernel<float, 4><<<blocks, 256, 0, st>>>((float*)d_X, ldx, (float*)d_Y, ldy, p, nA, q, d_U, u_f32,
+                                                          ldu, d_win, m);
+    else
+      maint_rows_kernel<float, 1><<<blocks, 256, 0, st>>>((float*)d_X, ldx, (float*)d_Y, ldy, p, nA, q, d_U, u_f32,
+                                                          ldu, d_win, m);
+  } else {
+    if (q % 2 == 0 && ldx % 2 == 0 && ldy % 2 == 0 && al % 16 == 0)
+      maint_rows_kernel<double, 2><<<blocks, 256, 0, st>>>((double*)d_X, ldx, (double*)d_Y, ldy, p, nA, q, d_U,
+                                                           u_f32, ldu, d_win, m);
+    else
+      maint_rows_kernel<double, 1><<<blocks, 256, 0, st>>>((double*)d_X, ldx, (double*)d_Y, ldy, p, nA, q, d_U,
+                                                           u_f32, ldu, d_win, m);
+  }
   rc = check_launch("maint_rows");
   if (rc) return rc;
   if (N > 0) {

@@ -62,7 +62,7 @@ template <typename T> struct SolvePrm {
   int *live, *pflag;
   T *ca, *cz, *cb;
   int* ctl;  // [0]=status [1]=err [2]=where [3]=any  [4..5]=barrier count/gen
-  long long* stats;  // [0]=iterations [1]=flushes
+  long long* stats;  // [0]=iterations [1]=flushes [2..7]=phase ns (CTA 0 view)
   uint64_t timeout_ns;
 };
 
@@ -105,39 +105,63 @@ POLAR_D void reduce_partials(const double* part, int nblk, int ld, double* tmp, 
 // ---------------------------------------------------------------------------------------
 template <typename T, int VEC, bool WEIGHTED>
 POLAR_D void spmm_phase(const polar_graph& g, const RowGroup& rg, int gid, int GT, double shift, const T* X,
-                        T* Y, int ld, typename AccOf<T>::type* chunk_part, int* hcount, double (&dacc)[VEC]) {
+                        T* Y, int ld, typename AccOf<T>::type* chunk_part, int* hcount, double (&dacc)[VEC],
+                        const int* act) {
   using A = typename AccOf<T>::type;
+  bool on = false;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) on |= act[rg.col + v] != 0;
+  // Heavy rows: each chunk adds its own share of d_i . v_i (-d_i . partial; the first
+  // chunk also the diagonal and added-edge terms) to the accumulator of the row group
+  // that owns the chunk.  Chunk -> row group is fixed, so the dot product does not depend
+  // on which group happens to finish the row.
   for (int ch = gid; ch < g.nchunks; ch += GT) {
     const int h = __ldg(g.d_chunk_row + ch);
     const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
+    const int i = __ldg(g.d_hrow + h);
+    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
     A acc[VEC];
 #pragma unroll
     for (int v = 0; v < VEC; ++v) acc[v] = A(0);
-    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc);
-    vstore<A, VEC>(chunk_part + (size_t)ch * ld + rg.col, acc);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc, on);
+    T xi[VEC];
+    if (on) {
+      vstore<A, VEC>(chunk_part + (size_t)ch * ld + rg.col, acc);
+      vload<T, VEC>(xi, X + (size_t)i * ld + rg.col);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
+    }
+    if (ch == c0 && on) {
+      A ex[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) ex[v] = A(0);
+      const double wadd = added_terms<T, VEC>(g, rg, i, X, ld, ex);
+      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+      const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v] - (double)ex[v]);
+    }
     __threadfence();
     __syncwarp(rg.mask);
     int old = 0;
     if (rg.lg == 0) old = atomicAdd(hcount + h, 1);
     old = __shfl_sync(rg.mask, old, 0, rg.G);
-    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
     if (old == c1 - c0 - 1) {
       __threadfence();
       A sum[VEC];
 #pragma unroll
       for (int v = 0; v < VEC; ++v) sum[v] = A(0);
-      for (int c2 = c0; c2 < c1; ++c2) {
-        A pv[VEC];
-        vload_cg<A, VEC>(pv, chunk_part + (size_t)c2 * ld + rg.col);
+      if (on) {
+        for (int c2 = c0; c2 < c1; ++c2) {
+          A pv[VEC];
+          vload_cg<A, VEC>(pv, chunk_part + (size_t)c2 * ld + rg.col);
 #pragma unroll
-        for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
+          for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
+        }
       }
-      const int i = __ldg(g.d_hrow + h);
       const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-      T xi[VEC], yi[VEC];
-      finish_row<T, VEC>(g, rg, i, deg, shift, X, ld, sum, Y, ld, xi, yi);
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+      T xf[VEC], yi[VEC];
+      finish_row<T, VEC>(g, rg, i, deg, shift, X, ld, sum, Y, ld, xf, yi, on);
       if (rg.lg == 0) hcount[h] = 0;
     }
   }
@@ -147,9 +171,9 @@ POLAR_D void spmm_phase(const polar_graph& g, const RowGroup& rg, int gid, int G
     A acc[VEC];
 #pragma unroll
     for (int v = 0; v < VEC; ++v) acc[v] = A(0);
-    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc, on);
     T xi[VEC], yi[VEC];
-    finish_row<T, VEC>(g, rg, i, hi - lo, shift, X, ld, acc, Y, ld, xi, yi);
+    finish_row<T, VEC>(g, rg, i, hi - lo, shift, X, ld, acc, Y, ld, xi, yi, on);
 #pragma unroll
     for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
   }
@@ -326,6 +350,16 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
   bool capped = false;
   bool more = ld_volatile_i32(P.ctl + 3) != 0 && P.maxit > 0;
   if (ld_volatile_i32(P.ctl + 3) != 0 && P.maxit <= 0) capped = true;
+  const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+  uint64_t tmark = timer ? globaltimer_ns() : 0;
+  auto lap = [&](int slot) {
+    if (timer) {
+      const uint64_t t = globaltimer_ns();
+      P.stats[2 + slot] += (long long)(t - tmark);
+      tmark = t;
+    }
+  };
+  lap(5);  // init (P0 + R0)
   while (more) {
     // ---- P4 (deferred shifted update of the previous M iterations) ----
     if (flush_pending) {
@@ -335,12 +369,13 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
       flush_pending = false;
       if (blockIdx.x == 0 && threadIdx.x == 0) P.stats[1] += 1;
     }
+    lap(0);
     // ---- P1 ----
     {
       double dacc[VEC];
 #pragma unroll
       for (int v = 0; v < VEC; ++v) dacc[v] = 0.0;
-      spmm_phase<T, VEC, WEIGHTED>(P.g, rg, gid, GT, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, dacc);
+      spmm_phase<T, VEC, WEIGHTED>(P.g, rg, gid, GT, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, dacc, P.act);
       reduce_cols_to_part<VEC>(dacc, rg.G, ld, red, my_part);
     }
     // ---- R1 ----
@@ -360,6 +395,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
         return;
       }
     }
+    lap(1);
     // ---- P2 ----
     {
       double a_c[VEC], racc[VEC];
@@ -439,6 +475,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
         return;
       }
     }
+    lap(2);
     const int any_after = ld_volatile_i32(P.ctl + 3);
     more = any_after && it + 1 < P.maxit;
     capped = any_after && !more;
@@ -515,9 +552,11 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
     ++it;
     flush_pending = pending == kHist;
     if (!grid_sync(gs, 4)) return;
+    lap(3);
   }
   // ---- final pass: remaining steps, X -> output ----
   shifted_update<T, E>(P, pending, first, true, tid, nth);
+  lap(4);
   if (blockIdx.x == 0) {
     if (P.track && P.h_out)
       for (int q = threadIdx.x; q < p * ld; q += blockDim.x) {
@@ -746,7 +785,7 @@ extern "C" int polar_msolve_finish(void* d_workspace, polar_stream_t stream, pol
   SolveRecord rec;
   if (!lookup_solve(d_workspace, &rec)) return set_error(POLAR_ERR_BAD_ARG, "no solve launched on this workspace");
   int ctl[4];
-  long long stats[2];
+  long long stats[8];
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMemcpyAsync(ctl, rec.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(stats, rec.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
@@ -762,6 +801,7 @@ extern "C" int polar_msolve_finish(void* d_workspace, polar_stream_t stream, pol
     info->flushes = stats[1];
     info->error_where = ctl[2];
     info->pad = 0;
+    for (int i = 0; i < 6; ++i) info->phase_ns[i] = stats[2 + i];
   }
   if (status == POLAR_ERR_ITER_CAP) return set_error(status, "multi-shift CG iteration cap");
   if (status == POLAR_ERR_NONFINITE) return set_error(status, "non-finite value in CG");

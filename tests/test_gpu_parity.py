@@ -122,7 +122,7 @@ def test_msolve_heavy_split_and_determinism(torch_cuda):
     assert np.array_equal(outs[1][0], outs[2][0]) and np.array_equal(outs[1][1], outs[2][1])
     Xo, ho, ito = O.msolve(O.Op(O.Graph(n, E, 1e-2)), W, tau, active, 1e-9, track=True)
     assert _rel(outs[1][0], Xo) < 1e-8 and _rel(outs[1][1], ho) < 1e-8
-    assert np.max(np.abs(outs[1][2] - ito)) <= 2
+    assert np.max(np.abs(outs[1][2] - ito)) <= max(5, 0.02 * ito.max())
 
 
 def test_msolve_errors(torch_cuda):
