@@ -53,7 +53,8 @@ enum polar_precision {
  * diagonal is (indptr[i+1]-indptr[i]) + sigma.  Added edges (Op.add) are a sorted list
  * of rows that carry extra neighbours (x_*), flagged in the bitset d_xbits.  Rows with
  * more than heavy_thresh neighbours are split into chunks (h_*), combined in a fixed
- * order so results are deterministic. */
+ * order so results are deterministic.  All other rows are covered by row blocks
+ * (d_rowblk): contiguous row ranges of bounded work that the SpMM streams through. */
 typedef struct polar_graph {
   int32_t n;
   int32_t nnz;
@@ -78,6 +79,9 @@ typedef struct polar_graph {
   const int32_t* d_chunk_row;  /* nchunks: heavy index */
   const int32_t* d_chunk_lo;   /* nchunks: first nnz position */
   const int32_t* d_chunk_hi;   /* nchunks: one past last */
+  /* light rows in contiguous blocks of roughly equal work (heavy rows excluded) */
+  int32_t nrb;
+  const int32_t* d_rowblk;     /* 2*nrb: [first row, one past last row] */
 } polar_graph;
 
 /* Statistics of the last solve (filled by polar_msolve_finish). */
@@ -128,6 +132,10 @@ int polar_msolve(const polar_graph* g, int precision, const double* d_W, int ldw
 int polar_msolve_finish(void* d_workspace, polar_stream_t stream, polar_msolve_info* info);
 /* Host-side limit for each grid-barrier wait inside polar_msolve (nanoseconds). */
 void polar_set_barrier_timeout_ns(uint64_t ns);
+/* Solver driver: 0 (default) one high-occupancy kernel per phase, M iterations per
+ * CUDA-graph launch, host checks convergence once per launch (polar_msolve then returns
+ * after the solve); 1: one persistent cooperative kernel with bounded grid barriers. */
+int polar_set_solver_mode(int mode);
 
 /* ---- incidence right-hand sides (polar_gpu.py:225-226, 282) ----
  * For c < R with e = sel[c] and (a, b) = cand[e] (cand: int64 [N][2]):

@@ -46,6 +46,7 @@ class PolarGraph(ctypes.Structure):
         ("heavy_thresh", ctypes.c_int32), ("nheavy", ctypes.c_int32), ("nchunks", ctypes.c_int32),
         ("d_hrow", ctypes.c_void_p), ("d_hchunk_off", ctypes.c_void_p), ("d_chunk_row", ctypes.c_void_p),
         ("d_chunk_lo", ctypes.c_void_p), ("d_chunk_hi", ctypes.c_void_p),
+        ("nrb", ctypes.c_int32), ("d_rowblk", ctypes.c_void_p),
     ]
 
 
@@ -73,6 +74,7 @@ SIGNATURES = {
     "polar_msolve": (_I, [_GP, _I, _P, _I, _I, _P, _I, _P, _P, _I, _D, _I64, _I, _P, _I, _I, _P, _P, _P, _S, _P]),
     "polar_msolve_finish": (_I, [_P, _P, ctypes.POINTER(MsolveInfo)]),
     "polar_set_barrier_timeout_ns": (None, [ctypes.c_uint64]),
+    "polar_set_solver_mode": (_I, [_I]),
     "polar_fill_incidence": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
     "polar_pair_norms": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _P]),
     "polar_topb_tmp_bytes": (_S, [_I, _I]),

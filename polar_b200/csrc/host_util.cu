@@ -29,7 +29,12 @@ void clear_error() { g_err.clear(); }
 
 void remember_solve(void* ws, int* ctl, long long* stats, int ld, int grid, int block) {
   std::lock_guard<std::mutex> lk(g_mu);
-  g_solves[ws] = SolveRecord{ctl, stats, ld, grid, block};
+  g_solves[ws] = SolveRecord{ctl, stats, ld, grid, block, false, 0, 0, 0};
+}
+
+void remember_solve_done(void* ws, int status, long long iterations, long long flushes, int ld, int grid, int block) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_solves[ws] = SolveRecord{nullptr, nullptr, ld, grid, block, true, status, iterations, flushes};
 }
 
 bool lookup_solve(void* ws, SolveRecord* out) {

@@ -12,8 +12,12 @@ struct SolveRecord {
   int* ctl;
   long long* stats;
   int ld, grid, block;
+  bool done;  // solve already completed on the host side (kernel-per-phase driver)
+  int status;
+  long long iterations, flushes;
 };
 void remember_solve(void* ws, int* ctl, long long* stats, int ld, int grid, int block);
+void remember_solve_done(void* ws, int status, long long iterations, long long flushes, int ld, int grid, int block);
 bool lookup_solve(void* ws, SolveRecord* out);
 
 }  // namespace polar

@@ -28,232 +28,10 @@
 #include "common.cuh"
 #include "graph_ops.cuh"
 #include "host_util.h"
+#include "solver_core.cuh"
+#include "msolve_mk.h"
 
 namespace polar {
-
-constexpr int kBlock = 512;
-constexpr int kWarps = kBlock / 32;
-constexpr int kMaxLd = 128;
-constexpr int kHist = 16;  // M: iterations per deferred shifted-update pass
-
-template <typename T> struct SolvePrm {
-  polar_graph g;
-  int n, R, ld, p, nA;
-  double tol;
-  long long maxit;
-  int track;
-  const double* W;
-  int ldw;
-  const double* tau;
-  const int* active;
-  const int* active_pos;
-  void* Xout;
-  int x_f32, ldx;
-  double* h_out;
-  long long* iters_out;
-  // workspace
-  T *r, *d, *v, *hist, *Pb, *Xb;
-  typename AccOf<T>::type* chunk_part;
-  int* hcount;
-  double* part;
-  double *rr, *stop, *ap, *bp, *ag, *beg, *chig;
-  int *act, *upd;
-  double *z, *zp, *hs, *ip, *pn;
-  int *live, *pflag;
-  T *ca, *cz, *cb;
-  int* ctl;  // [0]=status [1]=err [2]=where [3]=any  [4..5]=barrier count/gen
-  long long* stats;  // [0]=iterations [1]=flushes [2..7]=phase ns (CTA 0 view)
-  uint64_t timeout_ns;
-};
-
-// ---------------------------------------------------------------------------------------
-template <int VEC>
-POLAR_D void reduce_cols_to_part(double (&acc)[VEC], int G, int ld, double* red, double* out_row) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int o = G; o < 32; o <<= 1)
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
-  if (lane < G)
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) red[warp * ld + lane * VEC + v] = acc[v];
-  __syncthreads();
-  for (int c = threadIdx.x; c < ld; c += blockDim.x) {
-    double s = 0.0;
-    for (int w = 0; w < kWarps; ++w) s += red[w * ld + c];
-    out_row[c] = s;
-  }
-}
-
-// Sum of per-CTA partials part[b][c] over b in a fixed order (deterministic).
-POLAR_D void reduce_partials(const double* part, int nblk, int ld, double* tmp, double* out) {
-  const int S = blockDim.x / ld;
-  const int t = threadIdx.x, c = t % ld, s = t / ld;
-  if (s < S) {
-    double acc = 0.0;
-    for (int b = s; b < nblk; b += S) acc += __ldcg(part + (size_t)b * ld + c);
-    tmp[s * ld + c] = acc;
-  }
-  __syncthreads();
-  if (t < ld) {
-    double acc = 0.0;
-    for (int s2 = 0; s2 < S; ++s2) acc += tmp[s2 * ld + t];
-    out[t] = acc;
-  }
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------------------------------
-template <typename T, int VEC, bool WEIGHTED>
-POLAR_D void spmm_phase(const polar_graph& g, const RowGroup& rg, int gid, int GT, double shift, const T* X,
-                        T* Y, int ld, typename AccOf<T>::type* chunk_part, int* hcount, double (&dacc)[VEC],
-                        const int* act) {
-  using A = typename AccOf<T>::type;
-  bool on = false;
-#pragma unroll
-  for (int v = 0; v < VEC; ++v) on |= act[rg.col + v] != 0;
-  // Heavy rows: each chunk adds its own share of d_i . v_i (-d_i . partial; the first
-  // chunk also the diagonal and added-edge terms) to the accumulator of the row group
-  // that owns the chunk.  Chunk -> row group is fixed, so the dot product does not depend
-  // on which group happens to finish the row.
-  for (int ch = gid; ch < g.nchunks; ch += GT) {
-    const int h = __ldg(g.d_chunk_row + ch);
-    const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
-    const int i = __ldg(g.d_hrow + h);
-    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
-    A acc[VEC];
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
-    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc, on);
-    T xi[VEC];
-    if (on) {
-      vstore<A, VEC>(chunk_part + (size_t)ch * ld + rg.col, acc);
-      vload<T, VEC>(xi, X + (size_t)i * ld + rg.col);
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
-    }
-    if (ch == c0 && on) {
-      A ex[VEC];
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) ex[v] = A(0);
-      const double wadd = added_terms<T, VEC>(g, rg, i, X, ld, ex);
-      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-      const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v] - (double)ex[v]);
-    }
-    __threadfence();
-    __syncwarp(rg.mask);
-    int old = 0;
-    if (rg.lg == 0) old = atomicAdd(hcount + h, 1);
-    old = __shfl_sync(rg.mask, old, 0, rg.G);
-    if (old == c1 - c0 - 1) {
-      __threadfence();
-      A sum[VEC];
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) sum[v] = A(0);
-      if (on) {
-        for (int c2 = c0; c2 < c1; ++c2) {
-          A pv[VEC];
-          vload_cg<A, VEC>(pv, chunk_part + (size_t)c2 * ld + rg.col);
-#pragma unroll
-          for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
-        }
-      }
-      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-      T xf[VEC], yi[VEC];
-      finish_row<T, VEC>(g, rg, i, deg, shift, X, ld, sum, Y, ld, xf, yi, on);
-      if (rg.lg == 0) hcount[h] = 0;
-    }
-  }
-  for (int i = gid; i < g.n; i += GT) {
-    const int lo = __ldg(g.d_indptr + i), hi = __ldg(g.d_indptr + i + 1);
-    if (hi - lo > g.heavy_thresh) continue;
-    A acc[VEC];
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
-    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, X, ld, acc, on);
-    T xi[VEC], yi[VEC];
-    finish_row<T, VEC>(g, rg, i, hi - lo, shift, X, ld, acc, Y, ld, xi, yi, on);
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
-  }
-}
-
-// ---------------------------------------------------------------------------------------
-// Deferred shifted update over `nsteps` recorded iterations.  Thread item = (tile of E
-// active rows, column c); the E rows share the per-(pole, step, column) coefficients.
-template <typename T, int E>
-POLAR_D void shifted_update(const SolvePrm<T>& P, int nsteps, bool first, bool final_pass, long long tid,
-                            long long nth) {
-  const int ld = P.ld, nA = P.nA, p = P.p;
-  const int ntile = (nA + E - 1) / E;
-  const long long items = (long long)ntile * ld;
-  for (long long item = tid; item < items; item += nth) {
-    const int tile = (int)(item / ld), c = (int)(item % ld);
-    const int a0 = tile * E;
-    T hv[E][kHist];
-#pragma unroll
-    for (int e = 0; e < E; ++e)
-#pragma unroll
-      for (int k = 0; k < kHist; ++k)
-        hv[e][k] = (k < nsteps && a0 + e < nA) ? P.hist[((size_t)k * nA + a0 + e) * ld + c] : T(0);
-    T w0[E];
-    if (first) {
-#pragma unroll
-      for (int e = 0; e < E; ++e)
-        w0[e] = (a0 + e < nA && c < P.R) ? (T)__ldg(P.W + (size_t)__ldg(P.active + a0 + e) * P.ldw + c) : T(0);
-    }
-    for (int j = 0; j < p; ++j) {
-      const bool on = P.pflag[j * ld + c] != 0 && nsteps > 0;
-      if (!first && !final_pass && !on) continue;
-      const size_t base = ((size_t)j * nA + a0) * ld + c;
-      T x[E], pv[E];
-#pragma unroll
-      for (int e = 0; e < E; ++e) {
-        const bool ok = a0 + e < nA;
-        x[e] = first ? T(0) : (ok ? P.Xb[base + (size_t)e * ld] : T(0));
-        pv[e] = first ? w0[e] : ((on && ok) ? P.Pb[base + (size_t)e * ld] : T(0));
-      }
-      if (on) {
-#pragma unroll
-        for (int k = 0; k < kHist; ++k) {
-          if (k < nsteps) {
-            const size_t ci = ((size_t)k * p + j) * ld + c;
-            const T aj = P.ca[ci], zn = P.cz[ci], bj = P.cb[ci];
-            if (aj != T(0) || zn != T(0)) {
-#pragma unroll
-              for (int e = 0; e < E; ++e) {
-                x[e] = fma(aj, pv[e], x[e]);
-                pv[e] = fma(zn, hv[e][k], bj * pv[e]);
-              }
-            }
-          }
-        }
-        if (!final_pass) {
-#pragma unroll
-          for (int e = 0; e < E; ++e)
-            if (a0 + e < nA) P.Pb[base + (size_t)e * ld] = pv[e];
-        }
-      }
-      if (final_pass) {
-        if (c < P.R) {
-#pragma unroll
-          for (int e = 0; e < E; ++e) {
-            if (a0 + e < nA) {
-              const size_t o = ((size_t)j * nA + a0 + e) * P.ldx + c;
-              if (P.x_f32) reinterpret_cast<float*>(P.Xout)[o] = (float)x[e];
-              else reinterpret_cast<double*>(P.Xout)[o] = (double)x[e];
-            }
-          }
-        }
-      } else {
-#pragma unroll
-        for (int e = 0; e < E; ++e)
-          if (a0 + e < nA) P.Xb[base + (size_t)e * ld] = x[e];
-      }
-    }
-  }
-}
 
 // ---------------------------------------------------------------------------------------
 template <typename T, int VEC, bool WEIGHTED, int E>
@@ -371,13 +149,8 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
     }
     lap(0);
     // ---- P1 ----
-    {
-      double dacc[VEC];
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) dacc[v] = 0.0;
-      spmm_phase<T, VEC, WEIGHTED>(P.g, rg, gid, GT, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, dacc, P.act);
-      reduce_cols_to_part<VEC>(dacc, rg.G, ld, red, my_part);
-    }
+    spmm_phase<T, VEC, WEIGHTED, true>(P.g, ld, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, red, P.act);
+    reduce_red_to_part(red, ld, my_part);
     // ---- R1 ----
     {
       unsigned g1;
@@ -572,7 +345,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
 
 // ---------------------------------------------------------------------------------------
 struct SolveLayout {
-  size_t off[40];
+  size_t off[48];
   size_t total;
   int ld, vec;
 };
@@ -612,7 +385,7 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
   add((size_t)p * nA * ld * ts);                   // 4 P
   add((size_t)p * nA * ld * ts);                   // 5 X
   add((size_t)(g->nchunks > 0 ? g->nchunks : 1) * ld * ts);  // 6 chunk partials
-  add((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4);           // 7 heavy counters
+  add((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 * (ld > 16 ? ld / 16 : 1));  // 7 heavy counters per panel
   add((size_t)grid * ld * 8);                      // 8 CTA partials
   for (int i = 0; i < 6; ++i) add((size_t)ld * 8);  // 9..14 rr stop ap bp a be
   add((size_t)ld * 4);                             // 15 act
@@ -624,6 +397,8 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
   add(64);                                         // 27 ctl
   add(64);                                         // 28 stats
   add((size_t)ld * 8);                             // 29 chi
+  add(4096);                                       // 30 device copy of the parameter block
+  add((size_t)p * ld * kNC * 8);                   // 31 composed deferred-update coefficients
   L->total = o;
   L->ld = ld;
   L->vec = choose_vec(precision, ld);
@@ -651,18 +426,33 @@ static int max_grid_for(int precision, int vec, bool weighted) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int nb = 0;
   if (precision == POLAR_MIXED) {
-    if (vec == 4) nb = weighted ? occupancy_of<float, 4, true, 4>() : occupancy_of<float, 4, false, 4>();
-    else if (vec == 2) nb = weighted ? occupancy_of<float, 2, true, 4>() : occupancy_of<float, 2, false, 4>();
-    else nb = weighted ? occupancy_of<float, 1, true, 4>() : occupancy_of<float, 1, false, 4>();
+    if (vec == 4) nb = weighted ? occupancy_of<float, 4, true, POLAR_E32>() : occupancy_of<float, 4, false, POLAR_E32>();
+    else if (vec == 2) nb = weighted ? occupancy_of<float, 2, true, POLAR_E32>() : occupancy_of<float, 2, false, POLAR_E32>();
+    else nb = weighted ? occupancy_of<float, 1, true, POLAR_E32>() : occupancy_of<float, 1, false, POLAR_E32>();
   } else {
-    if (vec == 2) nb = weighted ? occupancy_of<double, 2, true, 2>() : occupancy_of<double, 2, false, 2>();
-    else nb = weighted ? occupancy_of<double, 1, true, 2>() : occupancy_of<double, 1, false, 2>();
+    if (vec == 2) nb = weighted ? occupancy_of<double, 2, true, POLAR_E64>() : occupancy_of<double, 2, false, POLAR_E64>();
+    else nb = weighted ? occupancy_of<double, 1, true, POLAR_E64>() : occupancy_of<double, 1, false, POLAR_E64>();
   }
   if (nb < 1) nb = 1;
   return nb * sms;
 }
 
 static uint64_t g_timeout_ns = 4000000000ull;  // 4 s per barrier wait
+static int g_solver_mode = 0;                      // 0: kernel-per-phase graph, 1: persistent
+
+template <typename T, int VEC, bool W, int E>
+static int mk_grid_for() { return mk_grid_max<T, VEC, W, E>(); }
+
+static int grid_for_mode(int precision, int vec, bool weighted) {
+  if (g_solver_mode == 1) return max_grid_for(precision, vec, weighted);
+  if (precision == POLAR_MIXED) {
+    if (vec == 4) return weighted ? mk_grid_for<float, 4, true, POLAR_E32>() : mk_grid_for<float, 4, false, POLAR_E32>();
+    if (vec == 2) return weighted ? mk_grid_for<float, 2, true, POLAR_E32>() : mk_grid_for<float, 2, false, POLAR_E32>();
+    return weighted ? mk_grid_for<float, 1, true, POLAR_E32>() : mk_grid_for<float, 1, false, POLAR_E32>();
+  }
+  if (vec == 2) return weighted ? mk_grid_for<double, 2, true, POLAR_E64>() : mk_grid_for<double, 2, false, POLAR_E64>();
+  return weighted ? mk_grid_for<double, 1, true, POLAR_E64>() : mk_grid_for<double, 1, false, POLAR_E64>();
+}
 
 }  // namespace polar
 
@@ -670,11 +460,17 @@ using namespace polar;
 
 extern "C" void polar_set_barrier_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 1; }
 
+extern "C" int polar_set_solver_mode(int mode) {
+  if (mode != 0 && mode != 1) return POLAR_ERR_BAD_ARG;
+  g_solver_mode = mode;
+  return POLAR_OK;
+}
+
 extern "C" size_t polar_msolve_workspace_bytes(const polar_graph* g, int precision, int R, int p, int nA) {
   if (!g || R < 1 || p < 1 || nA < 0) return 0;
   const int ld = choose_ld(precision, R);
   SolveLayout L;
-  solve_layout(g, precision, R, p, nA, max_grid_for(precision, choose_vec(precision, ld), g->d_wts != nullptr), &L);
+  solve_layout(g, precision, R, p, nA, grid_for_mode(precision, choose_vec(precision, ld), g->d_wts != nullptr), &L);
   return L.total;
 }
 
@@ -693,7 +489,7 @@ extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d
   const int ld = choose_ld(precision, R);
   const int vec = choose_vec(precision, ld);
   const bool weighted = g->d_wts != nullptr;
-  const int grid = max_grid_for(precision, vec, weighted);
+  const int grid = grid_for_mode(precision, vec, weighted);
   SolveLayout L;
   solve_layout(g, precision, R, p, nA, grid, &L);
   if (workspace_bytes < L.total) return set_error(POLAR_ERR_WORKSPACE, "workspace too small");
@@ -703,7 +499,7 @@ extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d
   cudaError_t e;
   e = cudaMemsetAsync(ws + L.off[27], 0, 64, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws + L.off[28], 0, 64, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(ws + L.off[7], 0, align256((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws + L.off[7], 0, L.off[8] - L.off[7], st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_iters_out, 0, sizeof(int64_t) * R, st);
   if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync", e);
 
@@ -759,20 +555,42 @@ extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d
     prm.ctl = (int*)(ws + L.off[27]);
     prm.stats = (long long*)(ws + L.off[28]);
     prm.chig = (double*)(ws + L.off[29]);
+    prm.cmp = g_solver_mode == 0 ? (double*)(ws + L.off[31]) : nullptr;
     prm.timeout_ns = g_timeout_ns;
   };
   int rc;
+  if (g_solver_mode == 0) {
+    MkResult res{};
+    if (precision == POLAR_MIXED) {
+      SolvePrm<float> prm;
+      fill(&prm);
+      SolvePrm<float>* dp = (SolvePrm<float>*)(ws + L.off[30]);
+      if (vec == 4) rc = weighted ? mk_solve<float, 4, true, POLAR_E32>(prm, dp, st, &res) : mk_solve<float, 4, false, POLAR_E32>(prm, dp, st, &res);
+      else if (vec == 2) rc = weighted ? mk_solve<float, 2, true, POLAR_E32>(prm, dp, st, &res) : mk_solve<float, 2, false, POLAR_E32>(prm, dp, st, &res);
+      else rc = weighted ? mk_solve<float, 1, true, POLAR_E32>(prm, dp, st, &res) : mk_solve<float, 1, false, POLAR_E32>(prm, dp, st, &res);
+    } else {
+      SolvePrm<double> prm;
+      fill(&prm);
+      SolvePrm<double>* dp = (SolvePrm<double>*)(ws + L.off[30]);
+      if (vec == 2) rc = weighted ? mk_solve<double, 2, true, POLAR_E64>(prm, dp, st, &res) : mk_solve<double, 2, false, POLAR_E64>(prm, dp, st, &res);
+      else rc = weighted ? mk_solve<double, 1, true, POLAR_E64>(prm, dp, st, &res) : mk_solve<double, 1, false, POLAR_E64>(prm, dp, st, &res);
+    }
+    if (rc != POLAR_OK) return rc;
+    const int status = res.err ? res.err : (res.capped ? (int)POLAR_ERR_ITER_CAP : 0);
+    remember_solve_done(d_workspace, status, res.iterations, res.flushes, ld, res.grid, kBlock);
+    return POLAR_OK;
+  }
   if (precision == POLAR_MIXED) {
     SolvePrm<float> prm;
     fill(&prm);
-    if (vec == 4) rc = weighted ? launch_solve<float, 4, true, 4>(prm, grid, st) : launch_solve<float, 4, false, 4>(prm, grid, st);
-    else if (vec == 2) rc = weighted ? launch_solve<float, 2, true, 4>(prm, grid, st) : launch_solve<float, 2, false, 4>(prm, grid, st);
-    else rc = weighted ? launch_solve<float, 1, true, 4>(prm, grid, st) : launch_solve<float, 1, false, 4>(prm, grid, st);
+    if (vec == 4) rc = weighted ? launch_solve<float, 4, true, POLAR_E32>(prm, grid, st) : launch_solve<float, 4, false, POLAR_E32>(prm, grid, st);
+    else if (vec == 2) rc = weighted ? launch_solve<float, 2, true, POLAR_E32>(prm, grid, st) : launch_solve<float, 2, false, POLAR_E32>(prm, grid, st);
+    else rc = weighted ? launch_solve<float, 1, true, POLAR_E32>(prm, grid, st) : launch_solve<float, 1, false, POLAR_E32>(prm, grid, st);
   } else {
     SolvePrm<double> prm;
     fill(&prm);
-    if (vec == 2) rc = weighted ? launch_solve<double, 2, true, 2>(prm, grid, st) : launch_solve<double, 2, false, 2>(prm, grid, st);
-    else rc = weighted ? launch_solve<double, 1, true, 2>(prm, grid, st) : launch_solve<double, 1, false, 2>(prm, grid, st);
+    if (vec == 2) rc = weighted ? launch_solve<double, 2, true, POLAR_E64>(prm, grid, st) : launch_solve<double, 2, false, POLAR_E64>(prm, grid, st);
+    else rc = weighted ? launch_solve<double, 1, true, POLAR_E64>(prm, grid, st) : launch_solve<double, 1, false, POLAR_E64>(prm, grid, st);
   }
   if (rc != POLAR_OK) return rc;
   // remember the control block location for polar_msolve_finish
@@ -784,6 +602,20 @@ extern "C" int polar_msolve_finish(void* d_workspace, polar_stream_t stream, pol
   clear_error();
   SolveRecord rec;
   if (!lookup_solve(d_workspace, &rec)) return set_error(POLAR_ERR_BAD_ARG, "no solve launched on this workspace");
+  if (rec.done) {
+    if (info) {
+      memset(info, 0, sizeof(*info));
+      info->status = rec.status;
+      info->ld = rec.ld;
+      info->grid = rec.grid;
+      info->block = rec.block;
+      info->iterations = rec.iterations;
+      info->flushes = rec.flushes;
+    }
+    if (rec.status == POLAR_ERR_ITER_CAP) return set_error(rec.status, "multi-shift CG iteration cap");
+    if (rec.status == POLAR_ERR_NONFINITE) return set_error(rec.status, "non-finite value in CG");
+    return rec.status;
+  }
   int ctl[4];
   long long stats[8];
   cudaStream_t st = (cudaStream_t)stream;

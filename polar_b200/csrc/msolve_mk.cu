@@ -1,0 +1,455 @@
+// Multi-kernel multi-shift CG (sm_100a): one high-occupancy kernel per phase; the host
+// queues M iterations plus the deferred shifted update, then checks convergence once.
+//
+// Per iteration (realworld/polar_gpu.py:100-125):
+//   mk_spmm   v = (M + tau_0 I) d, partial d.v per CTA; the last CTA to finish reduces
+//             the partials in a fixed order and writes a = rr / d.v
+//   mk_resid  r <- r - a v, r on the active rows -> history slot, partial r.r; the last
+//             CTA computes beta, chi and convergence for every column
+//   mk_dir    zeta recurrences / tracker / freezing for all (pole, column) items and the
+//             step coefficients; d <- r + beta d
+// and after M iterations (or convergence)
+//   mk_flush  deferred shifted update of X and P from the history (final pass writes
+//             the output block)
+// Kernels take SolvePrm by value in the constant parameter space (__grid_constant__), so
+// field reads are uniform constant loads that no store can alias.  Reductions are
+// deterministic (fixed grids, fixed summation order).
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "common.cuh"
+#include "graph_ops.cuh"
+#include "host_util.h"
+#include "msolve_mk.h"
+#include "solver_core.cuh"
+
+namespace polar {
+
+// ctl: [0] status [1] err [2] where [3] any [4] ran [5] nsteps [6] first
+//      [7] cnt_init [8] cnt_spmm [9] cnt_resid [10] cnt_dir [11] cnt_flush
+enum { C_STATUS = 0, C_ERR, C_WHERE, C_ANY, C_RAN, C_NSTEPS, C_FIRST, C_CNT0, C_CNT1, C_CNT3, C_CNT4, C_CNT5 };
+
+POLAR_D bool last_cta(int* cnt) {
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(cnt, 1);
+    s_last = (t == (int)gridDim.x - 1) ? 1 : 0;
+    if (s_last) {
+      *cnt = 0;
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return s_last != 0;
+}
+
+constexpr size_t kFlushSmemMax = 200 * 1024;
+
+POLAR_D bool solve_live(const int* ctl, const long long* stats, long long maxit) {
+  return ld_volatile_i32(ctl + C_ANY) != 0 && stats[0] < maxit && ld_volatile_i32(ctl + C_ERR) == 0;
+}
+
+// ---- init: r = d = W, r.r --------------------------------------------------------------
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolvePrm<T> P) {
+
+  __shared__ double red[kWarps * kMaxLd];
+  __shared__ double s_col[kMaxLd];
+  const int ld = P.ld;
+  const RowGroup rg = make_row_group<VEC>(ld);
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  const long long nvec = (long long)P.n * rg.G;
+  const int lgG = __ffs(rg.G) - 1;
+  double acc[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
+  for (long long e = tid; e < nvec; e += nth) {
+    const long long i = e >> lgG;
+    T w[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      const int c = rg.col + v;
+      w[v] = (c < P.R) ? (T)__ldg(P.W + (size_t)i * P.ldw + c) : T(0);
+      acc[v] += (double)w[v] * (double)w[v];
+    }
+    vstore<T, VEC>(P.r + (size_t)i * ld + rg.col, w);
+    vstore<T, VEC>(P.d + (size_t)i * ld + rg.col, w);
+  }
+  reduce_cols_to_part<VEC>(acc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
+  if (last_cta(P.ctl + C_CNT0)) {
+    reduce_partials(P.part, gridDim.x, ld, red, s_col);
+    const bool anyv = init_step(P, s_col);
+    if (threadIdx.x == 0) {
+      P.ctl[C_ANY] = anyv ? 1 : 0;
+      P.ctl[C_RAN] = 0;
+      P.ctl[C_NSTEPS] = 0;
+      P.ctl[C_FIRST] = 1;
+      P.stats[0] = 0;
+      P.stats[1] = 0;
+    }
+  }
+}
+
+// ---- v = (M + tau_0 I) d and d.v -------------------------------------------------------
+template <typename T, int VEC, bool WEIGHTED>
+__global__ void __launch_bounds__(kBlock) mk_spmm(const __grid_constant__ SolvePrm<T> P) {
+
+  if (!solve_live(P.ctl, P.stats, P.maxit)) return;
+  using A = typename AccOf<T>::type;
+  __shared__ double red[kWarps * kMaxLd];
+  __shared__ double s_col[kMaxLd];
+  const polar_graph& g = P.g;
+  const int ld = P.ld;
+  const double shift = __ldg(P.tau);
+  const RowGroup rg = make_row_group<VEC>(ld);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gpw = 32 / rg.G;
+  const int gid = (blockIdx.x * kWarps + warp) * gpw + lane / rg.G;
+  const int GT = gridDim.x * kWarps * gpw;
+  bool on = false;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) on |= P.act[rg.col + v] != 0;
+  double dacc[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) dacc[v] = 0.0;
+  // heavy rows, chunked (chunk -> row group fixed; each chunk adds its own share of d.v)
+  for (int ch = gid; ch < g.nchunks; ch += GT) {
+    const int h = __ldg(g.d_chunk_row + ch);
+    const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
+    const int i = __ldg(g.d_hrow + h);
+    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
+    A acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, P.d, ld, acc, on);
+    T xi[VEC];
+    if (on) {
+      vstore<A, VEC>(P.chunk_part + (size_t)ch * ld + rg.col, acc);
+      vload<T, VEC>(xi, P.d + (size_t)i * ld + rg.col);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
+      if (ch == c0) {
+        A ex[VEC];
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) ex[v] = A(0);
+        const double wadd = added_terms<T, VEC>(g, rg, i, P.d, ld, ex);
+        const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+        const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v] - (double)ex[v]);
+      }
+    }
+    __threadfence();
+    __syncwarp(rg.mask);
+    int old = 0;
+    if (rg.lg == 0) old = atomicAdd(P.hcount + h, 1);
+    old = __shfl_sync(rg.mask, old, 0, rg.G);
+    if (old == c1 - c0 - 1) {
+      __threadfence();
+      A sum[VEC];
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) sum[v] = A(0);
+      if (on)
+        for (int c2 = c0; c2 < c1; ++c2) {
+          A pv[VEC];
+          vload_cg<A, VEC>(pv, P.chunk_part + (size_t)c2 * ld + rg.col);
+#pragma unroll
+          for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
+        }
+      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+      T xf[VEC], yi[VEC];
+      finish_row<T, VEC>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
+      if (rg.lg == 0) P.hcount[h] = 0;
+    }
+  }
+  // light rows, one row group per row
+  for (int i = gid; i < g.n; i += GT) {
+    const int lo = __ldg(g.d_indptr + i), hi = __ldg(g.d_indptr + i + 1);
+    if (hi - lo > g.heavy_thresh) continue;
+    A acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
+    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, P.d, ld, acc, on);
+    T xi[VEC], yi[VEC];
+    finish_row<T, VEC>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+  }
+  reduce_cols_to_part<VEC>(dacc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
+  if (last_cta(P.ctl + C_CNT1)) {
+    reduce_partials(P.part, gridDim.x, ld, red, s_col);
+    for (int c = threadIdx.x; c < ld; c += blockDim.x) {
+      const int a_on = P.act[c];
+      const double a = a_on ? P.rr[c] / s_col[c] : 0.0;
+      if (a_on && !isfinite(a)) atomicCAS(P.ctl + C_ERR, 0, (int)POLAR_ERR_NONFINITE);
+      P.ag[c] = a;
+    }
+  }
+}
+
+// ---- r <- r - a v, history, r.r, column scalars -----------------------------------------
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kBlock) mk_resid(const __grid_constant__ SolvePrm<T> P, int slot) {
+
+  if (!solve_live(P.ctl, P.stats, P.maxit)) return;
+  __shared__ double red[kWarps * kMaxLd];
+  __shared__ double s_col[kMaxLd];
+  const int ld = P.ld, nA = P.nA;
+  const RowGroup rg = make_row_group<VEC>(ld);
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  const long long nvec = (long long)P.n * rg.G;
+  const int lgG = __ffs(rg.G) - 1;
+  double a_c[VEC], racc[VEC];
+  bool on[VEC], any_on = false;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) {
+    a_c[v] = P.ag[rg.col + v];
+    on[v] = P.act[rg.col + v] != 0;
+    any_on |= on[v];
+    racc[v] = 0.0;
+  }
+  if (any_on) {
+    T* hslot = P.hist + (size_t)slot * nA * ld;
+    constexpr int U = 2;
+    for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
+      T rv[U][VEC], vv[U][VEC];
+      long long ii[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const long long e = e0 + u * nth;
+        ii[u] = e < nvec ? (e >> lgG) : -1;
+        if (ii[u] >= 0) {
+          vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+          vload<T, VEC>(vv[u], P.v + (size_t)ii[u] * ld + rg.col);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (ii[u] < 0) continue;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) {
+          if (on[v]) rv[u][v] = (T)((double)rv[u][v] - a_c[v] * (double)vv[u][v]);
+          racc[v] += (double)rv[u][v] * (double)rv[u][v];
+        }
+        vstore<T, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
+        const int ai = __ldg(P.active_pos + ii[u]);
+        if (ai >= 0) vstore<T, VEC>(hslot + (size_t)ai * ld + rg.col, rv[u]);
+      }
+    }
+  }
+  reduce_cols_to_part<VEC>(racc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
+  if (last_cta(P.ctl + C_CNT3)) {
+    reduce_partials(P.part, gridDim.x, ld, red, s_col);
+    const bool anyv = column_step(P, s_col);
+    if (threadIdx.x == 0) {
+      P.ctl[C_ANY] = anyv ? 1 : 0;
+      P.ctl[C_RAN] = 1;
+      P.stats[0] += 1;
+    }
+  }
+}
+
+// ---- pole recurrences + d <- r + beta d -------------------------------------------------
+template <typename T, int VEC>
+__global__ void __launch_bounds__(kBlock) mk_dir(const __grid_constant__ SolvePrm<T> P, int slot) {
+
+  if (ld_volatile_i32(P.ctl + C_RAN) == 0) return;
+  const int ld = P.ld;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  const double shift0 = __ldg(P.tau);
+  for (long long q = tid; q < (long long)P.p * ld; q += nth) pole_step(P, q, slot, shift0);
+  const bool more = ld_volatile_i32(P.ctl + C_ANY) != 0 && P.stats[0] < P.maxit;
+  if (more) {
+    const RowGroup rg = make_row_group<VEC>(ld);
+    const long long nvec = (long long)P.n * rg.G;
+    const int lgG = __ffs(rg.G) - 1;
+    double be_c[VEC];
+    bool on[VEC], any_on = false;
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      be_c[v] = P.beg[rg.col + v];
+      on[v] = P.upd[rg.col + v] != 0;
+      any_on |= on[v];
+    }
+    if (any_on) {
+      constexpr int U = 2;
+      for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
+        T rv[U][VEC], dv[U][VEC];
+        long long ii[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const long long e = e0 + u * nth;
+          ii[u] = e < nvec ? (e >> lgG) : -1;
+          if (ii[u] >= 0) {
+            vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+            vload<T, VEC>(dv[u], P.d + (size_t)ii[u] * ld + rg.col);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (ii[u] < 0) continue;
+#pragma unroll
+          for (int v = 0; v < VEC; ++v)
+            if (on[v]) dv[u][v] = (T)((double)rv[u][v] + be_c[v] * (double)dv[u][v]);
+          vstore<T, VEC>(P.d + (size_t)ii[u] * ld + rg.col, dv[u]);
+        }
+      }
+    }
+  }
+  if (last_cta(P.ctl + C_CNT4)) {
+    if (threadIdx.x == 0) {
+      P.ctl[C_NSTEPS] = slot + 1;
+      P.ctl[C_RAN] = 0;
+    }
+  }
+}
+
+// ---- deferred shifted update (final pass writes the output) -----------------------------
+template <typename T, int E>
+__global__ void __launch_bounds__(kBlock, 2) mk_flush(const __grid_constant__ SolvePrm<T> P, int force_final) {
+  extern __shared__ __align__(16) unsigned char flush_sm[];
+
+  const int nsteps = ld_volatile_i32(P.ctl + C_NSTEPS);
+  const bool first = ld_volatile_i32(P.ctl + C_FIRST) != 0;
+  const bool done = ld_volatile_i32(P.ctl + C_ANY) == 0 || ld_volatile_i32(P.ctl + C_ERR) != 0;
+  const bool final_pass = force_final || done;
+  if (!final_pass && nsteps == 0) return;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  if (P.cmp && composed_smem_bytes<T>(P.ld, P.p) <= kFlushSmemMax)
+    shifted_update_composed<T, E>(P, nsteps, first, final_pass, reinterpret_cast<T*>(flush_sm));
+  else if (flush_smem_bytes<T>(P.ld, P.p, kHist) <= kFlushSmemMax)
+    shifted_update_smem<T, E>(P, nsteps, first, final_pass, reinterpret_cast<T*>(flush_sm));
+  else
+    shifted_update<T, E>(P, nsteps, first, final_pass, tid, nth);
+  if (final_pass && P.track && P.h_out)
+    for (long long q = tid; q < (long long)P.p * P.ld; q += nth) {
+      const int j = (int)(q / P.ld), c = (int)(q % P.ld);
+      if (c < P.R) P.h_out[(size_t)j * P.R + c] = P.hs[q];
+    }
+  if (last_cta(P.ctl + C_CNT5)) {
+    if (threadIdx.x == 0) {
+      P.ctl[C_NSTEPS] = 0;
+      P.ctl[C_FIRST] = 0;
+      P.stats[1] += 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+template <typename F>
+static int occ_grid(F* fn, int block) {
+  int dev = 0, sms = 0, nb = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0);
+  if (nb < 1) nb = 1;
+  return nb * sms;
+}
+
+template <typename T, int E>
+static size_t flush_smem_for(const SolvePrm<T>& P) {
+  if (P.cmp && composed_smem_bytes<T>(P.ld, P.p) <= kFlushSmemMax) return composed_smem_bytes<T>(P.ld, P.p);
+  const size_t b = flush_smem_bytes<T>(P.ld, P.p, kHist);
+  return b <= kFlushSmemMax ? b : 0;
+}
+
+template <typename T, int E>
+static int flush_grid(const SolvePrm<T>& P, size_t smem) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(mk_flush<T, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFlushSmemMax);
+    attr = true;
+  }
+  int dev = 0, sms = 0, nb = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mk_flush<T, E>, kBlock, smem);
+  if (nb < 1) nb = 1;
+  const int nch = P.ld / flush_cw<T>(P.ld);
+  int g = nb * sms;
+  g -= g % nch;
+  return g < nch ? nch : g;
+}
+
+template <typename T, int VEC, bool W, int E>
+int mk_grid_max() {
+  int g = occ_grid(mk_spmm<T, VEC, W>, kBlock);
+  g = g > occ_grid(mk_resid<T, VEC>, kBlock) ? g : occ_grid(mk_resid<T, VEC>, kBlock);
+  g = g > occ_grid(mk_init<T, VEC>, kBlock) ? g : occ_grid(mk_init<T, VEC>, kBlock);
+  return g;
+}
+
+template <typename T, int VEC, bool W, int E>
+int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
+  (void)dev_prm;
+  const int g0 = occ_grid(mk_init<T, VEC>, kBlock);
+  const int g1 = occ_grid(mk_spmm<T, VEC, W>, kBlock);
+  const int g3 = occ_grid(mk_resid<T, VEC>, kBlock);
+  const int g4 = occ_grid(mk_dir<T, VEC>, kBlock);
+  const size_t s5 = flush_smem_for<T, E>(P);
+  const int g5 = flush_grid<T, E>(P, s5);
+  // the composed flush multiplies every history slot (zero coefficients for unused ones)
+  cudaError_t e = cudaMemsetAsync(P.hist, 0, sizeof(T) * (size_t)kHist * P.nA * P.ld, st);
+  if (e != cudaSuccess) return set_cuda_error("history clear", e);
+  mk_init<T, VEC><<<g0, kBlock, 0, st>>>(P);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error("mk_init", e);
+  int ctl[8];
+  long long stats[2];
+  for (;;) {
+    // M iterations and one deferred-update pass; launches queue ahead of the device
+    for (int k = 0; k < kHist; ++k) {
+      mk_spmm<T, VEC, W><<<g1, kBlock, 0, st>>>(P);
+      mk_resid<T, VEC><<<g3, kBlock, 0, st>>>(P, k);
+      mk_dir<T, VEC><<<g4, kBlock, 0, st>>>(P, k);
+    }
+    mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error("msolve launch", e);
+    e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_cuda_error("msolve sync", e);
+    if (ctl[C_ERR] != 0 || ctl[C_ANY] == 0) break;
+    if (stats[0] >= P.maxit) {
+      mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 1);
+      e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return set_cuda_error("msolve sync", e);
+      break;
+    }
+  }
+  out->err = ctl[C_ERR];
+  out->capped = ctl[C_ERR] == 0 && ctl[C_ANY] != 0;
+  out->iterations = stats[0];
+  out->flushes = stats[1];
+  out->grid = g1;
+  return POLAR_OK;
+}
+
+#define POLAR_MK_INST(T, VEC, W, E)                                                                 \
+  template int mk_solve<T, VEC, W, E>(const SolvePrm<T>&, SolvePrm<T>*, cudaStream_t, MkResult*); \
+  template int mk_grid_max<T, VEC, W, E>();
+
+POLAR_MK_INST(float, 4, false, POLAR_E32)
+POLAR_MK_INST(float, 4, true, POLAR_E32)
+POLAR_MK_INST(float, 2, false, POLAR_E32)
+POLAR_MK_INST(float, 2, true, POLAR_E32)
+POLAR_MK_INST(float, 1, false, POLAR_E32)
+POLAR_MK_INST(float, 1, true, POLAR_E32)
+POLAR_MK_INST(double, 2, false, POLAR_E64)
+POLAR_MK_INST(double, 2, true, POLAR_E64)
+POLAR_MK_INST(double, 1, false, POLAR_E64)
+POLAR_MK_INST(double, 1, true, POLAR_E64)
+
+}  // namespace polar

@@ -12,6 +12,9 @@
 namespace polar {
 
 constexpr int kSpmmBlock = 256;
+#ifndef POLAR_PANEL_MINB
+#define POLAR_PANEL_MINB 1
+#endif
 
 template <typename T, int VEC, bool WEIGHTED>
 __global__ void __launch_bounds__(kSpmmBlock) spmm_kernel(polar_graph g, int R, int G, double shift, const T* X,
@@ -74,6 +77,15 @@ __global__ void __launch_bounds__(kSpmmBlock) spmm_kernel(polar_graph g, int R, 
   }
 }
 
+// Panel/stream path (same code as the solver's SpMM phase) for power-of-two R with
+// vector-aligned strides; persistent-size grid so panels sweep the GPU in step.
+template <typename T, int VEC, bool WEIGHTED>
+__global__ void __launch_bounds__(512, POLAR_PANEL_MINB) spmm_panel_kernel(polar_graph g, int R, double shift, const T* X, int ldx,
+                                                         T* Y, int ldy, typename AccOf<T>::type* part, int* hcount) {
+  (void)ldx;
+  spmm_phase<T, VEC, WEIGHTED, false>(g, R, shift, X, Y, ldy, part, hcount, nullptr, nullptr);
+}
+
 static int spmm_vec(int precision, int R, int ldx, int ldy, const void* X, const void* Y) {
   const int maxv = precision == POLAR_MIXED ? 4 : 2;
   const size_t es = precision == POLAR_MIXED ? 4 : 8;
@@ -83,6 +95,24 @@ static int spmm_vec(int precision, int R, int ldx, int ldy, const void* X, const
       return v;
   }
   return 1;
+}
+
+template <typename T, int VEC, bool W>
+static int launch_spmm_panel(const polar_graph& g, int R, double shift, const void* X, int ldx, void* Y, int ldy,
+                             void* scratch, cudaStream_t st) {
+  using A = typename AccOf<T>::type;
+  A* part = reinterpret_cast<A*>(scratch);
+  int* hcount = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) +
+                                       (((size_t)(g.nchunks > 0 ? g.nchunks : 1) * 128 * sizeof(A) + 255) & ~size_t(255)));
+  int dev = 0, sms = 0, nb = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, spmm_panel_kernel<T, VEC, W>, 512, 0);
+  if (nb < 1) nb = 1;
+  spmm_panel_kernel<T, VEC, W><<<nb * sms, 512, 0, st>>>(g, R, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error("spmm launch", e);
+  return POLAR_OK;
 }
 
 template <typename T, int VEC, bool W>
@@ -119,7 +149,7 @@ extern "C" size_t polar_spmm_scratch_bytes(const polar_graph* g, int precision, 
   if (!g) return 0;
   const size_t es = precision == POLAR_MIXED ? 4 : 8;
   const size_t part = (((size_t)(g->nchunks > 0 ? g->nchunks : 1) * 128 * es + 255) & ~size_t(255));
-  return part + (((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 + 255) & ~size_t(255));
+  return part + (((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 * 8 + 255) & ~size_t(255));
 }
 
 extern "C" int polar_spmm_scratch_init(const polar_graph* g, int precision, int R, void* d_scratch,
@@ -141,6 +171,13 @@ extern "C" int polar_spmm(const polar_graph* g, int precision, int R, double shi
   if ((g->d_wts == nullptr) != (g->d_diag == nullptr)) return set_error(POLAR_ERR_BAD_ARG, "weights and diag go together");
   const bool w = g->d_wts != nullptr;
   cudaStream_t st = (cudaStream_t)stream;
+  const bool pow2 = (R & (R - 1)) == 0;
+  if (pow2 && ldx == R && precision == POLAR_MIXED && vec == 4)
+    return w ? launch_spmm_panel<float, 4, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+             : launch_spmm_panel<float, 4, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
+  if (pow2 && ldx == R && precision == POLAR_FP64 && vec == 2)
+    return w ? launch_spmm_panel<double, 2, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
+             : launch_spmm_panel<double, 2, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);
   if (precision == POLAR_MIXED) {
     if (vec == 4) return w ? launch_spmm<float, 4, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)
                            : launch_spmm<float, 4, false>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st);

@@ -31,6 +31,34 @@ def _i32(x, dev):
     return torch.as_tensor(np.ascontiguousarray(x, dtype=np.int32)).to(dev)
 
 
+def row_blocks(indptr, heavy_thresh, row_cost=4, target=None):
+    """Contiguous blocks of light rows (degree <= heavy_thresh) with about `target` work
+    each, work = nnz + row_cost per row; heavy rows are never inside a block.  Returns
+    int32[nrb, 2] of [first row, one past last row]."""
+    deg = np.diff(indptr.astype(np.int64))
+    n = len(deg)
+    if n == 0:
+        return np.zeros((0, 2), np.int32)
+    light = deg <= heavy_thresh
+    cost = np.where(light, deg + row_cost, 0)
+    if target is None:
+        target = int(np.clip(cost.sum() / 30000.0, 32, 512))
+    run = np.cumsum(~light)                       # run id changes at every heavy row
+    cum = np.cumsum(cost) - cost                  # work before row i
+    run_start = np.zeros(run.max() + 2, np.int64)
+    first = np.r_[True, run[1:] != run[:-1]]
+    run_start[run[first]] = cum[first]
+    key = run * (1 << 40) + (cum - run_start[run]) // target
+    idx = np.flatnonzero(light)
+    if len(idx) == 0:
+        return np.zeros((0, 2), np.int32)
+    k = key[idx]
+    brk = np.r_[True, (k[1:] != k[:-1]) | (idx[1:] != idx[:-1] + 1)]
+    starts = idx[brk]
+    ends = np.r_[idx[np.flatnonzero(brk)[1:] - 1] + 1, idx[-1] + 1]
+    return np.stack([starts, ends], axis=1).astype(np.int32)
+
+
 class _HostM0:
     """Host FP64 CSR of M0 = diag(deg + sigma) - A with the `.get()` the drivers call
     (realworld/run_real.py:49 uses G.M0.get().toarray() for dense oracles)."""
@@ -122,6 +150,9 @@ class Graph:
         self.chunk_row = _i32(chunk_row if total else one, dev)
         self.chunk_lo = _i32(c_lo if total else one, dev)
         self.chunk_hi = _i32(c_hi if total else one, dev)
+        self.rowblk_h = row_blocks(self._indptr_h, self.heavy_thresh)
+        self.nrb = len(self.rowblk_h)
+        self.rowblk = _i32(self.rowblk_h.ravel() if self.nrb else np.zeros(2, np.int32), dev)
 
     def Lam(self, k):
         """Spectral upper bound sigma + 2 dmax + 4k (realworld/polar_gpu.py:59-60)."""
@@ -146,6 +177,8 @@ class Graph:
         s.d_chunk_row = self.chunk_row.data_ptr()
         s.d_chunk_lo = self.chunk_lo.data_ptr()
         s.d_chunk_hi = self.chunk_hi.data_ptr()
+        s.nrb = self.nrb
+        s.d_rowblk = self.rowblk.data_ptr()
         if extra is not None:
             extra.fill(s)
         return s

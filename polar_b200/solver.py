@@ -14,7 +14,14 @@ import torch
 
 from . import _lib
 
-__all__ = ["msolve", "Counter", "precision_code", "max_columns", "prepare_active"]
+__all__ = ["msolve", "Counter", "precision_code", "max_columns", "prepare_active", "set_solver_mode"]
+
+
+def set_solver_mode(mode):
+    """'graph' (default): one kernel per phase, M iterations per CUDA-graph launch;
+    'persistent': a single cooperative kernel with bounded grid barriers."""
+    code = {"graph": 0, "persistent": 1}[mode]
+    _lib.check(_lib.load().polar_set_solver_mode(code), "set_solver_mode")
 
 
 class Counter:

@@ -96,6 +96,25 @@ def test_msolve_fp64_matches_reference(gold, torch_cuda):
     assert it[3] == 0 and np.all(X[:, :, 3] == 0)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_msolve_persistent_driver(gold, torch_cuda, prec):
+    """The single-launch cooperative driver gives the same solves as the graph driver."""
+    import polar_b200 as pg
+    from polar_b200.solver import set_solver_mode
+    z, op = _ms_inputs(gold, pg)
+    tol = 1e-10 if prec == "fp64" else 1e-7
+    Xg, hg, itg = pg.msolve(op, z["ms_W"], z["ms_tau"], z["ms_active"], tol, track=True, precision=prec)
+    set_solver_mode("persistent")
+    try:
+        Xp, hp, itp = pg.msolve(op, z["ms_W"], z["ms_tau"], z["ms_active"], tol, track=True, precision=prec)
+    finally:
+        set_solver_mode("graph")
+    assert np.max(np.abs(itg - itp)) <= 3  # different reduction order
+    lim = 1e-8 if prec == "fp64" else 1e-5
+    assert _rel(Xp.cpu().numpy(), Xg.cpu().numpy()) < lim
+    assert _rel(hp.cpu().numpy(), hg.cpu().numpy()) < lim
+
+
 def test_msolve_mixed_close_to_reference(gold, torch_cuda):
     import polar_b200 as pg
     z, op = _ms_inputs(gold, pg)
@@ -140,8 +159,11 @@ def test_msolve_errors(torch_cuda):
     with pytest.raises(_lib.PolarError) as ei:
         pg.msolve(op, Wn, tau, z["ms_active"], 1e-10)
     assert ei.value.status == _lib.POLAR_ERR_NONFINITE
-    # a barrier wait that runs out returns TIMEOUT and leaves the context usable
+    # a grid-barrier wait of the persistent driver that runs out returns TIMEOUT and
+    # leaves the context usable
+    from polar_b200.solver import set_solver_mode
     lib = _lib.load()
+    set_solver_mode("persistent")
     lib.polar_set_barrier_timeout_ns(1)
     try:
         with pytest.raises(_lib.PolarError) as ei:
@@ -149,6 +171,7 @@ def test_msolve_errors(torch_cuda):
         assert ei.value.status == _lib.POLAR_ERR_TIMEOUT
     finally:
         lib.polar_set_barrier_timeout_ns(4_000_000_000)
+        set_solver_mode("graph")
     X, h, it = pg.msolve(op, W, tau, z["ms_active"], 1e-10, track=True)
     assert np.isfinite(X.cpu().numpy()).all()
 
@@ -187,7 +210,38 @@ def test_polar_sequence_matches_reference(gold, g2, name, prec):
         np.testing.assert_allclose(res["marginals"], z[key], rtol=tol)
     if prec == "fp64":
         np.testing.assert_array_equal(np.array([t["shortlist"] for t in trace]), z[f"run_{name}_shortlists"])
-        assert abs(res["spmv"] - int(z[f"run_{name}_spmv"])) <= 2 * cfg["k"] + 2
+        ref_spmv = int(z[f"run_{name}_spmv"])
+        assert abs(res["spmv"] - ref_spmv) <= max(2 * cfg["k"] + 2, 0.01 * ref_spmv)
+
+
+def _oracle_round_scores(G, cand, k, s, **kw):
+    """Oracle run that also returns the proxy scores of every round (the array the
+    reference ranks with argsort, realworld/polar_gpu.py:219-221)."""
+    rec = []
+    orig = np.argsort
+
+    def spy(a, *args, **kwargs):
+        rec.append(-np.array(a, copy=True))
+        return orig(a, *args, **kwargs)
+
+    np.argsort = spy
+    try:
+        res = O.polar(G, cand, k, s, **kw)
+    finally:
+        np.argsort = orig
+    return res, rec
+
+
+def assert_same_or_tied(seq, ref_seq, scores, rel_tie):
+    """Sequences agree up to the first difference; there the two picks' oracle scores
+    must agree within rel_tie (a tie the arithmetic cannot resolve)."""
+    for r, (a, b) in enumerate(zip(seq, ref_seq)):
+        if a != b:
+            sc = scores[r]
+            assert abs(sc[a] - sc[b]) <= rel_tie * abs(sc[b]), (r, a, b, sc[a], sc[b])
+            return r
+    assert len(seq) == len(ref_seq)
+    return None
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
@@ -199,10 +253,18 @@ def test_plain_workload_matches_reference(gold, torch_cuda, prec):
     G = pg.Graph(2000, E, 1e-2)
     sk = pg.sketches(G, cand, 32, 2026)
     res = pg.polar(G, cand, 10, 0.5, q=32, B=1, tol=1e-8, sketch=sk, K=16, precision=prec)
-    assert res["sequence"] == list(z["plain_sequence"])
-    ores = O.polar(O.Graph(2000, E, 1e-2), cand, 10, 0.5, q=32, B=1, tol=1e-8, sketch=sk, K=16)
-    tol = 1e-9 if prec == "fp64" else 1e-6
-    np.testing.assert_allclose(res["marginals"], ores["marginals"], rtol=tol)
+    ores, scores = _oracle_round_scores(O.Graph(2000, E, 1e-2), cand, 10, 0.5, q=32, B=1, tol=1e-8, sketch=sk,
+                                        K=16)
+    assert ores["sequence"] == list(z["plain_sequence"])
+    if prec == "fp64":
+        assert res["sequence"] == list(z["plain_sequence"])
+        np.testing.assert_allclose(res["marginals"], ores["marginals"], rtol=1e-9)
+    else:
+        # FP32 sketches resolve proxy scores to ~1e-7; round 10 of this workload is a
+        # 1.5e-12 near-tie (candidates 10624 / 10753) that only FP64 separates
+        r = assert_same_or_tied(res["sequence"], ores["sequence"], scores, 1e-6)
+        upto = len(res["sequence"]) if r is None else r
+        np.testing.assert_allclose(res["marginals"][:upto], ores["marginals"][:upto], rtol=1e-6)
 
 
 def test_true_marginals_match_reference(gold, g2):
