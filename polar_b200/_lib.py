@@ -67,6 +67,10 @@ _GP = ctypes.POINTER(PolarGraph)
 SIGNATURES = {
     "polar_last_error": (ctypes.c_char_p, []),
     "polar_version": (_I, []),
+    "polar_launch_count": (ctypes.c_longlong, []),
+    "polar_set_kernel_timing": (None, [_I]),
+    "polar_kernel_timing": (_I, [_I, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(ctypes.c_double)]),
     "polar_spmm_scratch_bytes": (_S, [_GP, _I, _I]),
     "polar_spmm_scratch_init": (_I, [_GP, _I, _I, _P, _P]),
     "polar_spmm": (_I, [_GP, _I, _I, _D, _P, _I, _P, _I, _P, _P]),
@@ -105,6 +109,22 @@ def load(path=None):
     if path is None:
         _lib = lib
     return lib
+
+
+KERNEL_CLASSES = {0: "spmm", 1: "resid", 2: "dir", 3: "flush", 4: "init"}
+
+
+def kernel_timing():
+    """{class name: (launches, device ms, algorithmic bytes)} since polar_set_kernel_timing(1)."""
+    lib = load()
+    out = {}
+    for cls, name in KERNEL_CLASSES.items():
+        n = ctypes.c_longlong()
+        ms = ctypes.c_double()
+        b = ctypes.c_double()
+        lib.polar_kernel_timing(cls, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(b))
+        out[name] = (n.value, ms.value, b.value)
+    return out
 
 
 def check(status, what=""):

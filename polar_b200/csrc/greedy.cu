@@ -385,6 +385,7 @@ __global__ void rank1_rows_kernel(double* F, int ldf, int q, const double* G, co
 }
 
 static int check_launch(const char* what) {
+  count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error(what, e);
   return POLAR_OK;

@@ -20,4 +20,19 @@ void remember_solve(void* ws, int* ctl, long long* stats, int ld, int grid, int 
 void remember_solve_done(void* ws, int status, long long iterations, long long flushes, int ld, int grid, int block);
 bool lookup_solve(void* ws, SolveRecord* out);
 
+// Kernel instrumentation: every launch of a libpolar kernel is counted; with timing on,
+// the solver's kernels are bracketed by CUDA events and their device time and
+// algorithmic bytes are accumulated per class.
+enum KernelClass { KC_SPMM = 0, KC_RESID, KC_DIR, KC_FLUSH, KC_INIT, KC_OTHER, KC_COUNT };
+void count_launch(int n = 1);
+bool timing_on();
+struct TimedLaunch {
+  int cls;
+  double bytes;
+  cudaEvent_t a, b;
+};
+cudaEvent_t timing_event();
+void timing_push(const TimedLaunch& t);
+void timing_collect();  // after a stream sync: fold finished pairs into the totals
+
 }  // namespace polar

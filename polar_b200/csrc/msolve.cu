@@ -409,6 +409,7 @@ static int launch_solve(const SolvePrm<T>& prm, int grid, cudaStream_t st) {
   void* args[] = {(void*)&prm};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)msolve_kernel<T, VEC, WEIGHTED, E>, dim3(grid),
                                               dim3(kBlock), args, 0, st);
+  count_launch();
   if (e != cudaSuccess) return set_cuda_error("cudaLaunchCooperativeKernel(msolve)", e);
   return POLAR_OK;
 }

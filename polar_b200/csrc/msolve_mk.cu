@@ -388,9 +388,31 @@ int mk_grid_max() {
   return g;
 }
 
+// Launch helper: counts the launch and, with timing on, brackets it with events and
+// records its algorithmic bytes.
+template <typename F>
+static void timed(int cls, double bytes, cudaStream_t st, F&& launch) {
+  count_launch();
+  if (!timing_on()) {
+    launch();
+    return;
+  }
+  TimedLaunch t{cls, bytes, timing_event(), timing_event()};
+  cudaEventRecord(t.a, st);
+  launch();
+  cudaEventRecord(t.b, st);
+  timing_push(t);
+}
+
 template <typename T, int VEC, bool W, int E>
 int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
   (void)dev_prm;
+  const double s = sizeof(T), n = P.n, R = P.R, nA = P.nA;
+  // algorithmic bytes per launch (unweighted CSR: values implicit, diagonal from indptr)
+  const double b_spmm = 4.0 * (n + 1) + 4.0 * P.g.nnz + 2.0 * s * n * R;
+  const double b_resid = 3.0 * s * n * R + s * nA * R;
+  const double b_dir = 3.0 * s * n * R;
+  const double b_flush = (4.0 * P.p + kHist) * s * nA * R;
   const int g0 = occ_grid(mk_init<T, VEC>, kBlock);
   const int g1 = occ_grid(mk_spmm<T, VEC, W>, kBlock);
   const int g3 = occ_grid(mk_resid<T, VEC>, kBlock);
@@ -400,7 +422,7 @@ int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResu
   // the composed flush multiplies every history slot (zero coefficients for unused ones)
   cudaError_t e = cudaMemsetAsync(P.hist, 0, sizeof(T) * (size_t)kHist * P.nA * P.ld, st);
   if (e != cudaSuccess) return set_cuda_error("history clear", e);
-  mk_init<T, VEC><<<g0, kBlock, 0, st>>>(P);
+  timed(KC_INIT, 2.0 * s * n * R + 8.0 * n * R, st, [&] { mk_init<T, VEC><<<g0, kBlock, 0, st>>>(P); });
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error("mk_init", e);
   int ctl[8];
@@ -408,20 +430,21 @@ int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResu
   for (;;) {
     // M iterations and one deferred-update pass; launches queue ahead of the device
     for (int k = 0; k < kHist; ++k) {
-      mk_spmm<T, VEC, W><<<g1, kBlock, 0, st>>>(P);
-      mk_resid<T, VEC><<<g3, kBlock, 0, st>>>(P, k);
-      mk_dir<T, VEC><<<g4, kBlock, 0, st>>>(P, k);
+      timed(KC_SPMM, b_spmm, st, [&] { mk_spmm<T, VEC, W><<<g1, kBlock, 0, st>>>(P); });
+      timed(KC_RESID, b_resid, st, [&] { mk_resid<T, VEC><<<g3, kBlock, 0, st>>>(P, k); });
+      timed(KC_DIR, b_dir, st, [&] { mk_dir<T, VEC><<<g4, kBlock, 0, st>>>(P, k); });
     }
-    mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 0);
+    timed(KC_FLUSH, b_flush, st, [&] { mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 0); });
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error("msolve launch", e);
     e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error("msolve sync", e);
+    if (timing_on()) timing_collect();
     if (ctl[C_ERR] != 0 || ctl[C_ANY] == 0) break;
     if (stats[0] >= P.maxit) {
-      mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 1);
+      timed(KC_FLUSH, b_flush, st, [&] { mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 1); });
       e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);

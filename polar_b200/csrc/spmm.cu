@@ -110,6 +110,7 @@ static int launch_spmm_panel(const polar_graph& g, int R, double shift, const vo
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, spmm_panel_kernel<T, VEC, W>, 512, 0);
   if (nb < 1) nb = 1;
   spmm_panel_kernel<T, VEC, W><<<nb * sms, 512, 0, st>>>(g, R, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount);
+  count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error("spmm launch", e);
   return POLAR_OK;
@@ -135,6 +136,7 @@ static int launch_spmm(const polar_graph& g, int R, double shift, const void* X,
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   spmm_kernel<T, VEC, W><<<(int)blocks, kSpmmBlock, 0, st>>>(g, R, G, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount);
+  count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error("spmm launch", e);
   return POLAR_OK;

@@ -111,6 +111,7 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
     cnt = Counter()
     live_h = np.ones(N, bool)
     seq, marg = [], []
+    solves = []  # (columns, seed iterations) of every multi-shift solve
     ph = _Phase(phases)
     wd = int(width) if width else min(2 * q, max_columns(prec))
     if wd > max_columns(prec):
@@ -122,8 +123,10 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
     def bank():
         for lo in range(0, 2 * q, wd):
             w = min(wd, 2 * q - lo)
+            inf = []
             msolve(op, RHS[:, lo:lo + w], tau_d, act_d, tol, maxit=maxit, counter=cnt, precision=prec, out=XY,
-                   out_col=lo, active_pos=pos_d)
+                   out_col=lo, active_pos=pos_d, info=inf)
+            solves.extend((w, int(i.iterations)) for i in inf)
         _lib.check(lib.polar_pair_norms(XY.data_ptr(), x_f32, p, nA, 2 * q, 0, q, ea_d.data_ptr(), eb_d.data_ptr(), N,
                                         h.data_ptr(), stream), "pair_norms")
         _lib.check(lib.polar_pair_norms(XY.data_ptr(), x_f32, p, nA, 2 * q, q, q, ea_d.data_ptr(), eb_d.data_ptr(), N,
@@ -154,8 +157,10 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
             _lib.check(lib.polar_fill_incidence(n, Br, cand_d.data_ptr(), short_d.data_ptr(), es_d.data_ptr(),
                                                 Wb.data_ptr(), Bmax, ia_d.data_ptr(), ib_d.data_ptr(), stream),
                        "fill_incidence")
+            inf = []
             Uv, hh, _ = msolve(op, Wb[:, :Br], tau_d, act_d, tol, maxit=maxit, track=(obj != "logdet"),
-                               counter=cnt, precision=prec, out=U, out_col=0, active_pos=pos_d)
+                               counter=cnt, precision=prec, out=U, out_col=0, active_pos=pos_d, info=inf)
+            solves.extend((Br, int(i.iterations)) for i in inf)
             ph.mark("select")
             _lib.check(lib.polar_rerank(U.data_ptr(), x_f32, p, nA, Bmax, ia_d.data_ptr(), ib_d.data_ptr(), Br,
                                         hh.data_ptr() if hh is not None else None, om_d.data_ptr(), ob,
@@ -183,7 +188,8 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
     _sync(dev)
     seconds = time.perf_counter() - t0
     out = dict(sequence=seq, seconds=seconds, spmv=cnt.spmv, rhs=cnt.rhs, p=p, rounds=len(seq),
-               truncated=len(seq) < k, marginals=marg, precision="mixed" if prec == _lib.POLAR_MIXED else "fp64")
+               truncated=len(seq) < k, marginals=marg, precision="mixed" if prec == _lib.POLAR_MIXED else "fp64",
+               solves=solves)
     if phases:
         out["phases"] = ph.summary()
     return out
