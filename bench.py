@@ -131,7 +131,8 @@ def build_inputs(a, rank=0):
     N = a.N or c["N"]
     k = a.k or c["k"]
     seed = c["seed"] + 1000 * rank
-    E = chung_lu(n, c["mean_deg"], c["gamma"], seed, dmax=c["dmax"] if n == c["n"] else None)
+    E = chung_lu(n, c["mean_deg"], c["gamma"], seed, dmax=c["dmax"] if n == c["n"] else None,
+                 min_degree=c.get("min_degree", 0))
     cand = candidates(n, E, N, seed + 7919)
     return dict(n=n, N=N, k=k, E=E, cand=cand, cfg=c, seed=seed)
 

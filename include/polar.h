@@ -82,6 +82,14 @@ typedef struct polar_graph {
   /* light rows in contiguous blocks of roughly equal work (heavy rows excluded) */
   int32_t nrb;
   const int32_t* d_rowblk;     /* 2*nrb: [first row, one past last row] */
+  /* optional sliced ELL of the light rows (unweighted graphs): slices of sell_s rows,
+   * sorted by degree; neighbour k of slice row r at sl_idx[sl_off[s] + k*sell_s + r],
+   * -1 pads; sl_rows[s*sell_s + r] = row id or -1.  nsl == 0: not provided. */
+  int32_t nsl;
+  int32_t sell_s;
+  const int32_t* d_sl_off;     /* nsl+1 */
+  const int32_t* d_sl_rows;    /* nsl*sell_s */
+  const int32_t* d_sl_idx;
 } polar_graph;
 
 /* Statistics of the last solve (filled by polar_msolve_finish). */
@@ -148,6 +156,18 @@ void polar_set_barrier_timeout_ns(uint64_t ns);
  * CUDA-graph launch, host checks convergence once per launch (polar_msolve then returns
  * after the solve); 1: one persistent cooperative kernel with bounded grid barriers. */
 int polar_set_solver_mode(int mode);
+/* Degree above which polar_msolve expects a row to be chunked for an R-column solve in
+ * this precision: 8 x (lanes per row).  Heavy rows are split into chunks of at most 256
+ * neighbours (polar_graph h_* fields), each processed by one warp. */
+int polar_heavy_threshold(int precision, int R);
+/* Rows per warp of the sliced-ELL layout polar_msolve uses for an R-column solve in this
+ * precision (0: it uses the CSR row loop). */
+int polar_sell_rows(int precision, int R);
+/* Bytes of each row that one lane of the solver's SpMM owns (16, 32 or 64; 0 = default 64).
+ * A row is processed by ld * element_size / bytes lanes. */
+void polar_set_spmm_lane_bytes(int bytes);
+/* 1 (default): polar_sell_rows reports the sliced-ELL height the solver uses; 0: CSR rows. */
+void polar_set_sell(int on);
 
 /* ---- incidence right-hand sides (polar_gpu.py:225-226, 282) ----
  * For c < R with e = sel[c] and (a, b) = cand[e] (cand: int64 [N][2]):

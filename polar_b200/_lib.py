@@ -47,6 +47,8 @@ class PolarGraph(ctypes.Structure):
         ("d_hrow", ctypes.c_void_p), ("d_hchunk_off", ctypes.c_void_p), ("d_chunk_row", ctypes.c_void_p),
         ("d_chunk_lo", ctypes.c_void_p), ("d_chunk_hi", ctypes.c_void_p),
         ("nrb", ctypes.c_int32), ("d_rowblk", ctypes.c_void_p),
+        ("nsl", ctypes.c_int32), ("sell_s", ctypes.c_int32),
+        ("d_sl_off", ctypes.c_void_p), ("d_sl_rows", ctypes.c_void_p), ("d_sl_idx", ctypes.c_void_p),
     ]
 
 
@@ -79,6 +81,10 @@ SIGNATURES = {
     "polar_msolve_finish": (_I, [_P, _P, ctypes.POINTER(MsolveInfo)]),
     "polar_set_barrier_timeout_ns": (None, [ctypes.c_uint64]),
     "polar_set_solver_mode": (_I, [_I]),
+    "polar_heavy_threshold": (_I, [_I, _I]),
+    "polar_sell_rows": (_I, [_I, _I]),
+    "polar_set_spmm_lane_bytes": (None, [_I]),
+    "polar_set_sell": (None, [_I]),
     "polar_fill_incidence": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
     "polar_pair_norms": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _P]),
     "polar_topb_tmp_bytes": (_S, [_I, _I]),

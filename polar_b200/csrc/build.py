@@ -62,7 +62,8 @@ def build(debug=False, verbose=False, out=OUT, extra=()):
     if not ok:
         raise RuntimeError("nvcc compilation failed")
     tmp = Path(str(out) + ".tmp")
-    link = [nvcc, "-shared", "-o", str(tmp)] + [str(o) for o in objs] + ARCH + ["-cudart", "static"]
+    link = [nvcc, "-shared", "-o", str(tmp)] + [str(o) for o in objs] + ARCH + ["-cudart", "static",
+                                                                                "-Xlinker", "--no-undefined"]
     subprocess.check_call(link)
     os.replace(tmp, out)
     return out

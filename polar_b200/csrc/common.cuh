@@ -25,29 +25,48 @@ union VecU {
   T a[V];
 };
 
+// Widest single access for V elements (at most 16 bytes); V elements are read as V / VW
+// such accesses when V * sizeof(T) exceeds 16 bytes.
+template <typename T, int V>
+struct VecWidth {
+  static constexpr int value = (V * (int)sizeof(T) <= 16) ? V : 16 / (int)sizeof(T);
+};
+
 template <typename T, int V>
 POLAR_D void vload(T (&out)[V], const T* p) {
-  VecU<T, V> u;
-  u.v = *reinterpret_cast<const typename VecType<T, V>::type*>(p);
+  constexpr int VW = VecWidth<T, V>::value;
 #pragma unroll
-  for (int i = 0; i < V; ++i) out[i] = u.a[i];
+  for (int c = 0; c < V / VW; ++c) {
+    VecU<T, VW> u;
+    u.v = *reinterpret_cast<const typename VecType<T, VW>::type*>(p + c * VW);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[c * VW + i] = u.a[i];
+  }
 }
 
 // L2-only load for data that other CTAs of the same persistent launch rewrite.
 template <typename T, int V>
 POLAR_D void vload_cg(T (&out)[V], const T* p) {
-  VecU<T, V> u;
-  u.v = __ldcg(reinterpret_cast<const typename VecType<T, V>::type*>(p));
+  constexpr int VW = VecWidth<T, V>::value;
 #pragma unroll
-  for (int i = 0; i < V; ++i) out[i] = u.a[i];
+  for (int c = 0; c < V / VW; ++c) {
+    VecU<T, VW> u;
+    u.v = __ldcg(reinterpret_cast<const typename VecType<T, VW>::type*>(p + c * VW));
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[c * VW + i] = u.a[i];
+  }
 }
 
 template <typename T, int V>
 POLAR_D void vstore(T* p, const T (&in)[V]) {
-  VecU<T, V> u;
+  constexpr int VW = VecWidth<T, V>::value;
 #pragma unroll
-  for (int i = 0; i < V; ++i) u.a[i] = in[i];
-  *reinterpret_cast<typename VecType<T, V>::type*>(p) = u.v;
+  for (int c = 0; c < V / VW; ++c) {
+    VecU<T, VW> u;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) u.a[i] = in[c * VW + i];
+    *reinterpret_cast<typename VecType<T, VW>::type*>(p + c * VW) = u.v;
+  }
 }
 
 // ---------------------------------------------------------------------------------------

@@ -45,11 +45,43 @@ POLAR_D RowGroup make_row_group(int ld) {
 
 // acc[v] += sum_{k in [lo,hi)} w_k * X[idx_k][col+v]
 // Lanes with on == false (all their columns converged) still take part in the index
-// shuffles but issue no loads.
+// shuffles but issue no loads.  Groups of 4+ lanes read a batch of G indices
+// cooperatively and broadcast them by shuffles; narrower groups read the next 4 indices
+// directly (the same addresses for the group's lanes, served by L1) so 4 gathers are in
+// flight per lane.
 template <typename T, int VEC, bool WEIGHTED>
 POLAR_D void gather_rows(const polar_graph& g, const RowGroup& rg, int lo, int hi, const T* X,
                          int ld, typename AccOf<T>::type (&acc)[VEC], bool on = true) {
   using A = typename AccOf<T>::type;
+  if (rg.G < 4) {
+    if (!on) return;
+    int k = lo;
+    for (; k + 4 <= hi; k += 4) {
+      int jj[4];
+      A ww[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        jj[u] = __ldg(g.d_indices + k + u);
+        ww[u] = WEIGHTED ? (A)__ldg(g.d_wts + k + u) : A(1);
+      }
+      T xv[4][VEC];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) vload<T, VEC>(xv[u], X + (size_t)jj[u] * ld + rg.col);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) acc[v] = WEIGHTED ? fma(ww[u], (A)xv[u][v], acc[v]) : acc[v] + (A)xv[u][v];
+    }
+    for (; k < hi; ++k) {
+      const int jj = __ldg(g.d_indices + k);
+      const A ww = WEIGHTED ? (A)__ldg(g.d_wts + k) : A(1);
+      T xv[VEC];
+      vload<T, VEC>(xv, X + (size_t)jj * ld + rg.col);
+#pragma unroll
+      for (int v = 0; v < VEC; ++v) acc[v] = WEIGHTED ? fma(ww, (A)xv[v], acc[v]) : acc[v] + (A)xv[v];
+    }
+    return;
+  }
   for (int k0 = lo; k0 < hi; k0 += rg.G) {
     const int k = k0 + rg.lg;
     int j = 0;
@@ -116,6 +148,24 @@ POLAR_D double added_terms(const polar_graph& g, const RowGroup& rg, int i, cons
     wsum += w;
   }
   return wsum;
+}
+
+// Finishes row i from its own entries xi (already loaded): y = (diag + shift) x_i - acc.
+template <typename T, int VEC>
+POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int deg, double shift, const T* X,
+                            int ld, typename AccOf<T>::type (&acc)[VEC], T* Y, int ldy, const T (&xi)[VEC],
+                            T (&yi)[VEC], bool store = true) {
+  using A = typename AccOf<T>::type;
+  if (!store) {
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) yi[v] = T(0);
+    return;
+  }
+  const double wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
+  const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) yi[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
+  vstore<T, VEC>(Y + (size_t)i * ldy + rg.col, yi);
 }
 
 // Finishes row i: y = (diag + shift) x_i - acc.  Returns x_i in xi (for d^T v).

@@ -461,6 +461,22 @@ using namespace polar;
 
 extern "C" void polar_set_barrier_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 1; }
 
+namespace polar {
+int mk_spmm_lanes(int precision, int ld);
+int mk_sell_rows(int precision, int ld);
+}
+
+extern "C" int polar_sell_rows(int precision, int R) {
+  if (g_solver_mode != 0) return 0;
+  return mk_sell_rows(precision, choose_ld(precision, R < 1 ? 1 : R));
+}
+
+extern "C" int polar_heavy_threshold(int precision, int R) {
+  const int ld = choose_ld(precision, R < 1 ? 1 : R);
+  const int G = g_solver_mode == 0 ? mk_spmm_lanes(precision, ld) : ld / choose_vec(precision, ld);
+  return 8 * G > 16 ? 8 * G : 16;
+}
+
 extern "C" int polar_set_solver_mode(int mode) {
   if (mode != 0 && mode != 1) return POLAR_ERR_BAD_ARG;
   g_solver_mode = mode;

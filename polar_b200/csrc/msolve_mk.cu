@@ -97,8 +97,12 @@ __global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolveP
 }
 
 // ---- v = (M + tau_0 I) d and d.v -------------------------------------------------------
-template <typename T, int VEC, bool WEIGHTED>
-__global__ void __launch_bounds__(kBlock) mk_spmm(const __grid_constant__ SolvePrm<T> P) {
+#ifndef POLAR_SPMM_MINB
+#define POLAR_SPMM_MINB 2  // resident 512-thread CTAs per SM requested for the SpMM kernel
+#endif
+// CPL: columns per lane (several 16-byte accesses when wider); row group = ld / CPL lanes.
+template <typename T, int CPL, bool W>
+__global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_constant__ SolvePrm<T> P) {
 
   if (!solve_live(P.ctl, P.stats, P.maxit)) return;
   using A = typename AccOf<T>::type;
@@ -107,81 +111,178 @@ __global__ void __launch_bounds__(kBlock) mk_spmm(const __grid_constant__ SolveP
   const polar_graph& g = P.g;
   const int ld = P.ld;
   const double shift = __ldg(P.tau);
-  const RowGroup rg = make_row_group<VEC>(ld);
+  const RowGroup rg = make_row_group<CPL>(ld);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gpw = 32 / rg.G;
   const int gid = (blockIdx.x * kWarps + warp) * gpw + lane / rg.G;
   const int GT = gridDim.x * kWarps * gpw;
   bool on = false;
 #pragma unroll
-  for (int v = 0; v < VEC; ++v) on |= P.act[rg.col + v] != 0;
-  double dacc[VEC];
+  for (int v = 0; v < CPL; ++v) on |= P.act[rg.col + v] != 0;
+  double dacc[CPL];
 #pragma unroll
-  for (int v = 0; v < VEC; ++v) dacc[v] = 0.0;
-  // heavy rows, chunked (chunk -> row group fixed; each chunk adds its own share of d.v)
-  for (int ch = gid; ch < g.nchunks; ch += GT) {
-    const int h = __ldg(g.d_chunk_row + ch);
-    const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
-    const int i = __ldg(g.d_hrow + h);
-    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
-    A acc[VEC];
+  for (int v = 0; v < CPL; ++v) dacc[v] = 0.0;
+  // heavy rows, chunked; one warp per chunk: the warp's row groups take interleaved
+  // neighbours and combine by shuffles in a fixed pattern (chunk -> warp fixed, so d.v
+  // does not depend on which warp finishes the row)
+  {
+    const int wid = blockIdx.x * kWarps + warp;
+    const int nw = gridDim.x * kWarps;
+    const int grp = lane / rg.G;
+    for (int ch = wid; ch < g.nchunks; ch += nw) {
+      const int h = __ldg(g.d_chunk_row + ch);
+      const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
+      const int i = __ldg(g.d_hrow + h);
+      const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
+      A acc[CPL];
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
-    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, P.d, ld, acc, on);
-    T xi[VEC];
-    if (on) {
-      vstore<A, VEC>(P.chunk_part + (size_t)ch * ld + rg.col, acc);
-      vload<T, VEC>(xi, P.d + (size_t)i * ld + rg.col);
+      for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+      for (int k0 = lo; k0 < hi; k0 += 32) {
+        const int k = k0 + lane;
+        int j = 0;
+        A w = A(1);
+        if (k < hi) {
+          j = __ldg(g.d_indices + k);
+          if (W) w = (A)__ldg(g.d_wts + k);
+        }
+        const int cnt = min(32, hi - k0);
+        for (int t0 = 0; t0 < cnt; t0 += 4 * gpw) {
+          T xv[4][CPL];
+          A ww[4];
+          bool okk[4];
 #pragma unroll
-      for (int v = 0; v < VEC; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
-      if (ch == c0) {
-        A ex[VEC];
+          for (int u = 0; u < 4; ++u) {
+            const int t = t0 + u * gpw + grp;
+            const int jt = __shfl_sync(0xffffffffu, j, t & 31);
+            ww[u] = W ? __shfl_sync(0xffffffffu, w, t & 31) : A(1);
+            okk[u] = t < cnt && on;
+            if (okk[u]) vload<T, CPL>(xv[u], P.d + (size_t)jt * ld + rg.col);
+          }
 #pragma unroll
-        for (int v = 0; v < VEC; ++v) ex[v] = A(0);
-        const double wadd = added_terms<T, VEC>(g, rg, i, P.d, ld, ex);
+          for (int u = 0; u < 4; ++u)
+            if (okk[u])
+#pragma unroll
+              for (int v = 0; v < CPL; ++v)
+                acc[v] = W ? fma(ww[u], (A)xv[u][v], acc[v]) : acc[v] + (A)xv[u][v];
+        }
+      }
+      for (int o = rg.G; o < 32; o <<= 1)
+#pragma unroll
+        for (int v = 0; v < CPL; ++v) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+      T xi[CPL];
+      if (on && grp == 0) {
+        vstore<A, CPL>(P.chunk_part + (size_t)ch * ld + rg.col, acc);
+        vload<T, CPL>(xi, P.d + (size_t)i * ld + rg.col);
+#pragma unroll
+        for (int v = 0; v < CPL; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
+        if (ch == c0) {
+          A ex[CPL];
+#pragma unroll
+          for (int v = 0; v < CPL; ++v) ex[v] = A(0);
+          const double wadd = added_terms<T, CPL>(g, rg, i, P.d, ld, ex);
+          const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+          const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
+#pragma unroll
+          for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v] - (double)ex[v]);
+        }
+      }
+      __threadfence();
+      __syncwarp();
+      int old = 0;
+      if (lane == 0) old = atomicAdd(P.hcount + h, 1);
+      old = __shfl_sync(0xffffffffu, old, 0);
+      if (old == c1 - c0 - 1 && grp == 0) {
+        __threadfence();
+        A sum[CPL];
+#pragma unroll
+        for (int v = 0; v < CPL; ++v) sum[v] = A(0);
+        if (on)
+          for (int c2 = c0; c2 < c1; ++c2) {
+            A pv[CPL];
+            vload_cg<A, CPL>(pv, P.chunk_part + (size_t)c2 * ld + rg.col);
+#pragma unroll
+            for (int v = 0; v < CPL; ++v) sum[v] += pv[v];
+          }
         const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-        const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
+        T xf[CPL], yi[CPL];
+        finish_row<T, CPL>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
+        if (lane == 0) P.hcount[h] = 0;
+      }
+      __syncwarp();
+    }
+  }
+  if (g.nsl > 0 && g.sell_s == gpw && !W) {
+    // light rows in sliced ELL: a warp takes a slice of gpw degree-sorted rows and reads
+    // neighbour k of all its rows with one coalesced load
+    const int wid = blockIdx.x * kWarps + warp;
+    const int nw = gridDim.x * kWarps;
+    const int grp = lane / rg.G;
+    const int S = gpw;
+    for (int sl = wid; sl < g.nsl; sl += nw) {
+      const int off = __ldg(g.d_sl_off + sl);
+      const int w = (__ldg(g.d_sl_off + sl + 1) - off) / S;
+      const int row = __ldg(g.d_sl_rows + sl * S + grp);
+      const bool valid = row >= 0;
+      const bool go = valid && on;
+      T xi[CPL], yi[CPL];
+      int deg = 0;
+      if (valid) deg = __ldg(g.d_indptr + row + 1) - __ldg(g.d_indptr + row);
+      if (go) vload<T, CPL>(xi, P.d + (size_t)row * ld + rg.col);
+      A acc[CPL];
 #pragma unroll
-        for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v] - (double)ex[v]);
+      for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+      const int* sp = g.d_sl_idx + off + grp;
+      int k = 0;
+      for (; k + 4 <= w; k += 4) {
+        int jj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) jj[u] = __ldg(sp + (k + u) * S);
+        T xv[4][CPL];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (go && jj[u] >= 0) vload<T, CPL>(xv[u], P.d + (size_t)jj[u] * ld + rg.col);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (go && jj[u] >= 0)
+#pragma unroll
+            for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
+      }
+      for (; k < w; ++k) {
+        const int jj = __ldg(sp + k * S);
+        if (go && jj >= 0) {
+          T xv[CPL];
+          vload<T, CPL>(xv, P.d + (size_t)jj * ld + rg.col);
+#pragma unroll
+          for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[v];
+        }
+      }
+      if (valid) {
+        finish_row_pre<T, CPL>(g, rg, row, deg, shift, P.d, ld, acc, P.v, ld, xi, yi, go);
+        if (go)
+#pragma unroll
+          for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
       }
     }
-    __threadfence();
-    __syncwarp(rg.mask);
-    int old = 0;
-    if (rg.lg == 0) old = atomicAdd(P.hcount + h, 1);
-    old = __shfl_sync(rg.mask, old, 0, rg.G);
-    if (old == c1 - c0 - 1) {
-      __threadfence();
-      A sum[VEC];
-#pragma unroll
-      for (int v = 0; v < VEC; ++v) sum[v] = A(0);
-      if (on)
-        for (int c2 = c0; c2 < c1; ++c2) {
-          A pv[VEC];
-          vload_cg<A, VEC>(pv, P.chunk_part + (size_t)c2 * ld + rg.col);
-#pragma unroll
-          for (int v = 0; v < VEC; ++v) sum[v] += pv[v];
-        }
-      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-      T xf[VEC], yi[VEC];
-      finish_row<T, VEC>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
-      if (rg.lg == 0) P.hcount[h] = 0;
+  } else {
+    // light rows, one row group per row; the row's own entries are loaded with its indices
+    for (int i = gid; i < g.n; i += GT) {
+      const int lo = __ldg(g.d_indptr + i), hi = __ldg(g.d_indptr + i + 1);
+      if (hi - lo > g.heavy_thresh) continue;
+      T xi[CPL], yi[CPL];
+      if (on) vload<T, CPL>(xi, P.d + (size_t)i * ld + rg.col);
+      A acc[CPL];
+  #pragma unroll
+      for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+      gather_rows<T, CPL, W>(g, rg, lo, hi, P.d, ld, acc, on);
+      finish_row_pre<T, CPL>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
+      if (!on)
+  #pragma unroll
+        for (int v = 0; v < CPL; ++v) xi[v] = T(0);
+  #pragma unroll
+      for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
     }
   }
-  // light rows, one row group per row
-  for (int i = gid; i < g.n; i += GT) {
-    const int lo = __ldg(g.d_indptr + i), hi = __ldg(g.d_indptr + i + 1);
-    if (hi - lo > g.heavy_thresh) continue;
-    A acc[VEC];
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) acc[v] = A(0);
-    gather_rows<T, VEC, WEIGHTED>(g, rg, lo, hi, P.d, ld, acc, on);
-    T xi[VEC], yi[VEC];
-    finish_row<T, VEC>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
-#pragma unroll
-    for (int v = 0; v < VEC; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
-  }
-  reduce_cols_to_part<VEC>(dacc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
+  reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
   if (last_cta(P.ctl + C_CNT1)) {
     reduce_partials(P.part, gridDim.x, ld, red, s_col);
     for (int c = threadIdx.x; c < ld; c += blockDim.x) {
@@ -195,7 +296,7 @@ __global__ void __launch_bounds__(kBlock) mk_spmm(const __grid_constant__ SolveP
 
 // ---- r <- r - a v, history, r.r, column scalars -----------------------------------------
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kBlock) mk_resid(const __grid_constant__ SolvePrm<T> P, int slot) {
+__global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ SolvePrm<T> P, int slot) {
 
   if (!solve_live(P.ctl, P.stats, P.maxit)) return;
   __shared__ double red[kWarps * kMaxLd];
@@ -258,7 +359,7 @@ __global__ void __launch_bounds__(kBlock) mk_resid(const __grid_constant__ Solve
 
 // ---- pole recurrences + d <- r + beta d -------------------------------------------------
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kBlock) mk_dir(const __grid_constant__ SolvePrm<T> P, int slot) {
+__global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ SolvePrm<T> P, int slot) {
 
   if (ld_volatile_i32(P.ctl + C_RAN) == 0) return;
   const int ld = P.ld;
@@ -346,6 +447,70 @@ __global__ void __launch_bounds__(kBlock, 2) mk_flush(const __grid_constant__ So
 
 // ---------------------------------------------------------------------------------------
 template <typename F>
+static int occ_grid(F* fn, int block);
+
+// SpMM launch for a runtime choice of columns per lane.
+template <typename T, bool W>
+struct SpmmLaunch {
+  template <int CPL>
+  static int grid() { return occ_grid(mk_spmm<T, CPL, W>, kBlock); }
+  template <int CPL>
+  static void go(int g, const SolvePrm<T>& P, cudaStream_t st) { mk_spmm<T, CPL, W><<<g, kBlock, 0, st>>>(P); }
+};
+
+static int g_spmm_cpl_bytes = 0;  // 0: automatic
+
+template <typename T>
+static int spmm_cpl(int ld, int vec) {
+  // 32 bytes per lane for rows of 512 bytes or more, otherwise one 16-byte access
+  int bytes = g_spmm_cpl_bytes ? g_spmm_cpl_bytes : (ld * (int)sizeof(T) >= 512 ? 32 : 16);
+  int cpl = bytes / (int)sizeof(T);
+  if (cpl < vec) cpl = vec;
+  if (cpl > ld) cpl = ld;
+  while (ld / cpl > 32) cpl *= 2;
+  return cpl;
+}
+
+static int g_sell = 1;
+int mk_spmm_lanes(int precision, int ld);
+
+int mk_sell_rows(int precision, int ld) {
+  if (!g_sell) return 0;
+  return 32 / mk_spmm_lanes(precision, ld);
+}
+
+int mk_spmm_lanes(int precision, int ld) {
+  if (precision == POLAR_MIXED) return ld / spmm_cpl<float>(ld, ld >= 4 ? 4 : ld);
+  return ld / spmm_cpl<double>(ld, ld >= 2 ? 2 : ld);
+}
+
+template <typename T, bool W>
+static int spmm_grid(int cpl) {
+  using L = SpmmLaunch<T, W>;
+  switch (cpl) {
+    case 1: return L::template grid<1>();
+    case 2: return L::template grid<2>();
+    case 4: return L::template grid<4>();
+    case 8: return L::template grid<8>();
+    default: return sizeof(T) == 4 ? L::template grid<16>() : L::template grid<8>();
+  }
+}
+
+template <typename T, bool W>
+static void spmm_go(int cpl, int g, const SolvePrm<T>& P, cudaStream_t st) {
+  using L = SpmmLaunch<T, W>;
+  switch (cpl) {
+    case 1: L::template go<1>(g, P, st); break;
+    case 2: L::template go<2>(g, P, st); break;
+    case 4: L::template go<4>(g, P, st); break;
+    case 8: L::template go<8>(g, P, st); break;
+    default:
+      if (sizeof(T) == 4) L::template go<16>(g, P, st);
+      else L::template go<8>(g, P, st);
+  }
+}
+
+template <typename F>
 static int occ_grid(F* fn, int block) {
   int dev = 0, sms = 0, nb = 0;
   cudaGetDevice(&dev);
@@ -382,7 +547,11 @@ static int flush_grid(const SolvePrm<T>& P, size_t smem) {
 
 template <typename T, int VEC, bool W, int E>
 int mk_grid_max() {
-  int g = occ_grid(mk_spmm<T, VEC, W>, kBlock);
+  int g = 0;
+  for (int cpl = 1; cpl <= 16 / (int)(sizeof(T) / 4); cpl *= 2) {
+    const int gc = spmm_grid<T, W>(cpl);
+    g = g > gc ? g : gc;
+  }
   g = g > occ_grid(mk_resid<T, VEC>, kBlock) ? g : occ_grid(mk_resid<T, VEC>, kBlock);
   g = g > occ_grid(mk_init<T, VEC>, kBlock) ? g : occ_grid(mk_init<T, VEC>, kBlock);
   return g;
@@ -414,7 +583,8 @@ int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResu
   const double b_dir = 3.0 * s * n * R;
   const double b_flush = (4.0 * P.p + kHist) * s * nA * R;
   const int g0 = occ_grid(mk_init<T, VEC>, kBlock);
-  const int g1 = occ_grid(mk_spmm<T, VEC, W>, kBlock);
+  const int cpl = spmm_cpl<T>(P.ld, VEC);
+  const int g1 = spmm_grid<T, W>(cpl);
   const int g3 = occ_grid(mk_resid<T, VEC>, kBlock);
   const int g4 = occ_grid(mk_dir<T, VEC>, kBlock);
   const size_t s5 = flush_smem_for<T, E>(P);
@@ -430,7 +600,7 @@ int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResu
   for (;;) {
     // M iterations and one deferred-update pass; launches queue ahead of the device
     for (int k = 0; k < kHist; ++k) {
-      timed(KC_SPMM, b_spmm, st, [&] { mk_spmm<T, VEC, W><<<g1, kBlock, 0, st>>>(P); });
+      timed(KC_SPMM, b_spmm, st, [&] { spmm_go<T, W>(cpl, g1, P, st); });
       timed(KC_RESID, b_resid, st, [&] { mk_resid<T, VEC><<<g3, kBlock, 0, st>>>(P, k); });
       timed(KC_DIR, b_dir, st, [&] { mk_dir<T, VEC><<<g4, kBlock, 0, st>>>(P, k); });
     }
@@ -459,6 +629,13 @@ int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResu
   out->grid = g1;
   return POLAR_OK;
 }
+
+}  // namespace polar
+
+extern "C" void polar_set_spmm_lane_bytes(int bytes) { polar::g_spmm_cpl_bytes = bytes; }
+extern "C" void polar_set_sell(int on) { polar::g_sell = on; }
+
+namespace polar {
 
 #define POLAR_MK_INST(T, VEC, W, E)                                                                 \
   template int mk_solve<T, VEC, W, E>(const SolvePrm<T>&, SolvePrm<T>*, cudaStream_t, MkResult*); \

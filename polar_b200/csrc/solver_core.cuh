@@ -327,8 +327,17 @@ POLAR_HD size_t composed_smem_bytes(int ld, int p) {
   return (size_t)p * kNC * flush_cw<T>(ld) * sizeof(T);
 }
 
+#ifndef POLAR_FLUSH_F64
+#define POLAR_FLUSH_F64 0  // 1: FP32 iterates are updated with FP64 arithmetic in the flush
+#endif
+template <typename T> struct FlushAcc { using type = T; };
+#if POLAR_FLUSH_F64
+template <> struct FlushAcc<float> { using type = double; };
+#endif
+
 template <typename T, int E>
 POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool first, bool final_pass, T* sm) {
+  using C = typename FlushAcc<T>::type;
   const int ld = P.ld, nA = P.nA, p = P.p;
   const int cw = flush_cw<T>(ld);
   const int nch = ld / cw;
@@ -380,21 +389,27 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
       if (!first && !final_pass && !on) return;
       if (on) {
         const T* cf = sm + (size_t)j * kNC * cw + cl;
-        const T alpha = cf[0], beta = cf[cw];
+        const C alpha = (C)cf[0], beta = (C)cf[cw];
+        C xc[E], pc[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-          const T p0 = pv[e];
-          x[e] = fma(alpha, p0, x[e]);
-          pv[e] = beta * p0;
+          const C p0 = (C)pv[e];
+          xc[e] = fma(alpha, p0, (C)x[e]);
+          pc[e] = beta * p0;
         }
 #pragma unroll
         for (int k = 0; k < kHist; ++k) {
-          const T gk = cf[(2 + k) * cw], dk = cf[(2 + kHist + k) * cw];
+          const C gk = (C)cf[(2 + k) * cw], dk = (C)cf[(2 + kHist + k) * cw];
 #pragma unroll
           for (int e = 0; e < E; ++e) {
-            x[e] = fma(gk, hv[e][k], x[e]);
-            pv[e] = fma(dk, hv[e][k], pv[e]);
+            xc[e] = fma(gk, (C)hv[e][k], xc[e]);
+            pc[e] = fma(dk, (C)hv[e][k], pc[e]);
           }
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          x[e] = (T)xc[e];
+          pv[e] = (T)pc[e];
         }
         if (!final_pass)
 #pragma unroll

@@ -31,6 +31,40 @@ def _i32(x, dev):
     return torch.as_tensor(np.ascontiguousarray(x, dtype=np.int32)).to(dev)
 
 
+def sell_slices(indptr, indices, light_mask, S, window=4096):
+    """Sliced ELL of the light rows for warps of S rows: rows are sorted by degree
+    (descending) within windows of `window` rows, cut into slices of S rows, and each
+    slice stores its neighbour lists column-major (index k of row r at off + k*S + r),
+    padded with -1 to the slice's largest degree.  Returns (slice_off int32[ns+1],
+    slice_rows int32[ns*S] (-1 pads), sidx int32)."""
+    rows = np.flatnonzero(light_mask).astype(np.int64)
+    if len(rows) == 0:
+        return np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32)
+    deg = (indptr[rows + 1] - indptr[rows]).astype(np.int64)
+    win = np.arange(len(rows)) // window
+    order = np.lexsort((-deg, win))
+    rows = rows[order]
+    deg = deg[order]
+    ns = -(-len(rows) // S)
+    pad = ns * S - len(rows)
+    rows_p = np.r_[rows, -np.ones(pad, np.int64)].reshape(ns, S)
+    deg_p = np.r_[deg, np.zeros(pad, np.int64)].reshape(ns, S)
+    width = deg_p.max(axis=1)
+    off = np.zeros(ns + 1, np.int64)
+    off[1:] = np.cumsum(width * S)
+    sidx = -np.ones(int(off[-1]), np.int64)
+    # position of neighbour k of slice row r: off[s] + k*S + r
+    rr = np.repeat(np.arange(ns * S), deg_p.ravel())
+    s_of = rr // S
+    r_in = rr % S
+    k_in = np.arange(len(rr)) - np.repeat(np.cumsum(deg_p.ravel()) - deg_p.ravel(), deg_p.ravel())
+    src = np.repeat(indptr[np.maximum(rows_p.ravel(), 0)].astype(np.int64), deg_p.ravel()) + k_in
+    sidx[off[s_of] + k_in * S + r_in] = indices[src]
+    if off[-1] >= 2 ** 31:
+        raise ValueError("sliced ELL too large for int32 offsets")
+    return off.astype(np.int32), rows_p.ravel().astype(np.int32), sidx.astype(np.int32)
+
+
 def row_blocks(indptr, heavy_thresh, row_cost=4, target=None):
     """Contiguous blocks of light rows (degree <= heavy_thresh) with about `target` work
     each, work = nnz + row_cost per row; heavy rows are never inside a block.  Returns
@@ -127,11 +161,27 @@ class Graph:
         self._split_heavy(int(heavy_thresh))
 
     # -- heavy-row split ---------------------------------------------------------------
+    CHUNK = 256  # neighbours per heavy-row chunk (one warp per chunk in the solver)
+
     def _split_heavy(self, thresh):
+        """Default partition (threshold `thresh`) plus a cache of partitions for other
+        thresholds: rows with more than `thresh` neighbours are cut into chunks of at most
+        CHUNK, combined in chunk order by the kernels."""
         self.heavy_thresh = max(1, thresh)
+        self._heavy = {}
+        hv = self._heavy_parts(self.heavy_thresh)
+        self.nheavy, self.nchunks = hv["nheavy"], hv["nchunks"]
+        self.hrow, self.hchunk_off = hv["hrow"], hv["hchunk_off"]
+        self.chunk_row, self.chunk_lo, self.chunk_hi = hv["chunk_row"], hv["chunk_lo"], hv["chunk_hi"]
+        self.rowblk_h, self.nrb, self.rowblk = hv["rowblk_h"], hv["nrb"], hv["rowblk"]
+
+    def _heavy_parts(self, thresh):
+        if thresh in self._heavy:
+            return self._heavy[thresh]
+        ch = min(self.CHUNK, max(1, thresh)) if thresh < self.CHUNK else self.CHUNK
         degs = np.diff(self._indptr_h.astype(np.int64))
-        hrow = np.flatnonzero(degs > self.heavy_thresh).astype(np.int32)
-        nch = -(-degs[hrow] // self.heavy_thresh) if len(hrow) else np.zeros(0, np.int64)
+        hrow = np.flatnonzero(degs > thresh).astype(np.int32)
+        nch = -(-degs[hrow] // ch) if len(hrow) else np.zeros(0, np.int64)
         off = np.zeros(len(hrow) + 1, np.int64)
         off[1:] = np.cumsum(nch)
         total = int(off[-1])
@@ -139,28 +189,52 @@ class Graph:
         within = np.arange(total, dtype=np.int64) - np.repeat(off[:-1], nch)
         lo = self._indptr_h[hrow].astype(np.int64)
         hi = self._indptr_h[hrow + 1].astype(np.int64) if len(hrow) else np.zeros(0, np.int64)
-        c_lo = np.repeat(lo, nch) + within * self.heavy_thresh
-        c_hi = np.minimum(c_lo + self.heavy_thresh, np.repeat(hi, nch))
+        c_lo = np.repeat(lo, nch) + within * ch
+        c_hi = np.minimum(c_lo + ch, np.repeat(hi, nch))
         dev = self.device
-        self.nheavy = len(hrow)
-        self.nchunks = total
         one = np.zeros(1, np.int32)
-        self.hrow = _i32(hrow if len(hrow) else one, dev)
-        self.hchunk_off = _i32(off, dev)
-        self.chunk_row = _i32(chunk_row if total else one, dev)
-        self.chunk_lo = _i32(c_lo if total else one, dev)
-        self.chunk_hi = _i32(c_hi if total else one, dev)
-        self.rowblk_h = row_blocks(self._indptr_h, self.heavy_thresh)
-        self.nrb = len(self.rowblk_h)
-        self.rowblk = _i32(self.rowblk_h.ravel() if self.nrb else np.zeros(2, np.int32), dev)
+        rb = row_blocks(self._indptr_h, thresh)
+        hv = dict(thresh=thresh, nheavy=len(hrow), nchunks=total, rowblk_h=rb, nrb=len(rb),
+                  rowblk=_i32(rb.ravel() if len(rb) else np.zeros(2, np.int32), dev),
+                  hrow=_i32(hrow if len(hrow) else one, dev), hchunk_off=_i32(off, dev),
+                  chunk_row=_i32(chunk_row if total else one, dev), chunk_lo=_i32(c_lo if total else one, dev),
+                  chunk_hi=_i32(c_hi if total else one, dev))
+        self._heavy[thresh] = hv
+        return hv
 
     def Lam(self, k):
         """Spectral upper bound sigma + 2 dmax + 4k (realworld/polar_gpu.py:59-60)."""
         return self.sigma + 2.0 * self.dmax + 4.0 * k
 
-    def struct(self, extra=None):
-        """ctypes polar_graph for this graph (plus an Op's added edges)."""
+    def _sell(self, thresh, S):
+        key = (thresh, S)
+        if not hasattr(self, "_sell_cache"):
+            self._sell_cache = {}
+        if key not in self._sell_cache:
+            degs = np.diff(self._indptr_h.astype(np.int64))
+            off, rows, sidx = sell_slices(self._indptr_h, self._indices_h, degs <= thresh, S)
+            dev = self.device
+            self._sell_cache[key] = dict(ns=len(off) - 1, off=_i32(off, dev),
+                                         rows=_i32(rows if len(rows) else np.zeros(1, np.int32), dev),
+                                         idx=_i32(sidx if len(sidx) else np.zeros(1, np.int32), dev))
+        return self._sell_cache[key]
+
+    def struct(self, extra=None, heavy_thresh=None, sell_rows=0):
+        """ctypes polar_graph for this graph (plus an Op's added edges), with the heavy-row
+        partition for `heavy_thresh` (default: the graph's own threshold) and, when
+        sell_rows > 0 (unweighted graphs), the sliced-ELL layout of the light rows for
+        warps of sell_rows rows."""
+        hv = self._heavy_parts(self.heavy_thresh if heavy_thresh is None else int(heavy_thresh))
         s = _lib.PolarGraph()
+        s.nsl = 0
+        s.sell_s = 0
+        if sell_rows and not self.weighted:
+            sl = self._sell(hv["thresh"], int(sell_rows))
+            s.nsl = sl["ns"]
+            s.sell_s = int(sell_rows)
+            s.d_sl_off = sl["off"].data_ptr()
+            s.d_sl_rows = sl["rows"].data_ptr()
+            s.d_sl_idx = sl["idx"].data_ptr()
         s.n = self.n
         s.nnz = self.nnz
         s.d_indptr = self.indptr.data_ptr()
@@ -169,16 +243,16 @@ class Graph:
         s.d_diag = self.diag.data_ptr() if self.weighted else None
         s.sigma = self.sigma
         s.nx = 0
-        s.heavy_thresh = self.heavy_thresh
-        s.nheavy = self.nheavy
-        s.nchunks = self.nchunks
-        s.d_hrow = self.hrow.data_ptr()
-        s.d_hchunk_off = self.hchunk_off.data_ptr()
-        s.d_chunk_row = self.chunk_row.data_ptr()
-        s.d_chunk_lo = self.chunk_lo.data_ptr()
-        s.d_chunk_hi = self.chunk_hi.data_ptr()
-        s.nrb = self.nrb
-        s.d_rowblk = self.rowblk.data_ptr()
+        s.heavy_thresh = hv["thresh"]
+        s.nheavy = hv["nheavy"]
+        s.nchunks = hv["nchunks"]
+        s.d_hrow = hv["hrow"].data_ptr()
+        s.d_hchunk_off = hv["hchunk_off"].data_ptr()
+        s.d_chunk_row = hv["chunk_row"].data_ptr()
+        s.d_chunk_lo = hv["chunk_lo"].data_ptr()
+        s.d_chunk_hi = hv["chunk_hi"].data_ptr()
+        s.nrb = hv["nrb"]
+        s.d_rowblk = hv["rowblk"].data_ptr()
         if extra is not None:
             extra.fill(s)
         return s
@@ -254,8 +328,8 @@ class Op:
         self.B.append(b)
         self._added.add(a, b, float(w))
 
-    def struct(self):
-        return self.G.struct(self._added)
+    def struct(self, heavy_thresh=None, sell_rows=0):
+        return self.G.struct(self._added, heavy_thresh=heavy_thresh, sell_rows=sell_rows)
 
     def __call__(self, x, shift=0.0):
         """Apply to an (n, R) or (n,) float64/float32 CUDA tensor; returns a new tensor."""

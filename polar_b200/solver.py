@@ -110,13 +110,13 @@ def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, *, 
     h = torch.zeros((p, R), dtype=torch.float64, device=dev) if track else None
     iters = torch.zeros(R, dtype=torch.int64, device=dev)
     lib = _lib.load()
-    g = op.struct()
     stream = torch.cuda.current_stream(dev).cuda_stream
     maxc = max_columns(prec)
     info_list = []
     for lo in range(0, R, maxc):
         hi = min(R, lo + maxc)
         r = hi - lo
+        g = op.struct(heavy_thresh=lib.polar_heavy_threshold(prec, r), sell_rows=lib.polar_sell_rows(prec, r))
         need = lib.polar_msolve_workspace_bytes(g, prec, r, p, nA)
         ws = workspace(need, dev)
         hpart = torch.zeros((p, r), dtype=torch.float64, device=dev) if track else None

@@ -39,7 +39,7 @@ def _chung_lu_weights(n, mean_deg, gamma, dmax):
     return w * (total / w.sum())
 
 
-def chung_lu(n, mean_deg, gamma, seed, dmax=None, m=None):
+def chung_lu(n, mean_deg, gamma, seed, dmax=None, m=None, min_degree=0):
     """Undirected simple Chung–Lu graph on vertices 0..n-1 (hubs at low ids).
 
     Endpoints are drawn independently with probability proportional to the expected
@@ -47,7 +47,10 @@ def chung_lu(n, mean_deg, gamma, seed, dmax=None, m=None):
     the same preprocessing rule as realworld/graphs.py:52-53 (sort each pair, drop u==v,
     unique).  Sampling repeats until exactly `m` distinct edges exist (default
     round(n*mean_deg/2)); a final seeded subset trims any overshoot.
-    Returns int64[m, 2] with u < v, rows sorted lexicographically."""
+    With min_degree=1, every vertex left isolated gets one edge to a partner drawn in
+    proportion to expected degree (the SNAP graphs these stand in for contain only
+    endpoint vertices, realworld/graphs.py:51); the edge count then grows by the number of
+    such vertices.  Returns int64[m', 2] with u < v, rows sorted lexicographically."""
     rng = np.random.default_rng(seed)
     w = _chung_lu_weights(n, mean_deg, gamma, dmax)
     target = int(round(n * mean_deg / 2)) if m is None else int(m)
@@ -65,6 +68,18 @@ def chung_lu(n, mean_deg, gamma, seed, dmax=None, m=None):
         keys = np.unique(np.concatenate([keys, a[keep] * n + b[keep]]))
     if len(keys) > target:
         keys = keys[np.sort(rng.choice(len(keys), target, replace=False))]
+    if min_degree >= 1:
+        deg = np.bincount(np.r_[keys // n, keys % n], minlength=n)
+        iso = np.flatnonzero(deg == 0)
+        if len(iso):
+            part = np.searchsorted(cdf, rng.random(len(iso)), side="right").clip(0, n - 1)
+            clash = part == iso
+            while clash.any():
+                part[clash] = np.searchsorted(cdf, rng.random(int(clash.sum())), side="right").clip(0, n - 1)
+                clash = part == iso
+            a = np.minimum(iso, part).astype(np.int64)
+            b = np.maximum(iso, part).astype(np.int64)
+            keys = np.unique(np.concatenate([keys, a * n + b]))
     return np.stack([keys // n, keys % n], axis=1).astype(np.int64)
 
 
@@ -99,13 +114,13 @@ def candidates(n, edges, N, seed):
 # Workload shapes.  Each entry: graph (n, mean degree, exponent, seed, dmax), pool size N,
 # pole count K, sketch width q, shortlist B, rounds k, sigma, s, CG tolerance.
 CONFIGS = {
-    "plain-n2000": dict(n=2000, mean_deg=6.0, gamma=2.5, seed=0, dmax=None, N=20000,
+    "plain-n2000": dict(n=2000, mean_deg=6.0, gamma=2.5, seed=0, dmax=None, min_degree=1, N=20000,
                         K=16, q=32, B=1, k=10, sigma=1e-2, s=0.5, tol=1e-8),
-    "precision-n317k": dict(n=317080, mean_deg=2 * 1049866 / 317080, gamma=2.4, seed=1, dmax=None,
+    "precision-n317k": dict(n=317080, mean_deg=2 * 1049866 / 317080, gamma=2.4, seed=1, dmax=None, min_degree=1,
                             N=200000, K=24, q=64, B=16, k=50, sigma=1e-2, s=0.5, tol=1e-7),
-    "diff-n1.13M": dict(n=1134890, mean_deg=2 * 2987624 / 1134890, gamma=2.2, seed=3, dmax=None,
+    "diff-n1.13M": dict(n=1134890, mean_deg=2 * 2987624 / 1134890, gamma=2.2, seed=3, dmax=None, min_degree=1,
                         N=4096, K=24, q=64, B=16, k=0, sigma=1e-2, s=0.5, tol=1e-7),
-    "full-n4M": dict(n=3997962, mean_deg=2 * 34681189 / 3997962, gamma=2.1, seed=4, dmax=15000,
+    "full-n4M": dict(n=3997962, mean_deg=2 * 34681189 / 3997962, gamma=2.1, seed=4, dmax=15000, min_degree=1,
                      N=1000000, K=32, q=64, B=16, k=100, sigma=1e-2, s=0.5, tol=1e-6),
 }
 
@@ -117,7 +132,7 @@ def make_config(name, n=None, N=None, cand_seed=None):
     n = c["n"] if n is None else int(n)
     N = c["N"] if N is None else int(N)
     dmax = c["dmax"] if n == c["n"] else None
-    edges = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=dmax)
+    edges = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=dmax, min_degree=c.get("min_degree", 0))
     seed = c["seed"] + 7919 if cand_seed is None else cand_seed
     cand = candidates(n, edges, N, seed)
     return edges, n, cand, c

@@ -138,7 +138,7 @@ meta["runs"] = runs
 
 # 5. plain workload at n=2000 (K=16, q=32, B=1, k=10, tol 1e-8, sigma 1e-2, s 0.5) ----------
 n3 = 2000
-E3 = chung_lu(n3, 6.0, 2.5, 0)
+E3 = chung_lu(n3, 6.0, 2.5, 0, min_degree=1)
 cand3 = ref_graphs.candidates(n3, E3, 20000, 0 + 7919)
 G3 = ref.Graph(n3, E3, 1e-2)
 sk3 = ref.sketches(G3, cand3, 32, 2026)

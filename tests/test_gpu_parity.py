@@ -248,7 +248,7 @@ def assert_same_or_tied(seq, ref_seq, scores, rel_tie):
 def test_plain_workload_matches_reference(gold, torch_cuda, prec):
     import polar_b200 as pg
     z, _ = gold
-    E = chung_lu(2000, 6.0, 2.5, 0)
+    E = chung_lu(2000, 6.0, 2.5, 0, min_degree=1)
     cand = candidates(2000, E, 20000, 7919)
     G = pg.Graph(2000, E, 1e-2)
     sk = pg.sketches(G, cand, 32, 2026)
@@ -260,8 +260,8 @@ def test_plain_workload_matches_reference(gold, torch_cuda, prec):
         assert res["sequence"] == list(z["plain_sequence"])
         np.testing.assert_allclose(res["marginals"], ores["marginals"], rtol=1e-9)
     else:
-        # FP32 sketches resolve proxy scores to ~1e-7; round 10 of this workload is a
-        # 1.5e-12 near-tie (candidates 10624 / 10753) that only FP64 separates
+        # FP32 sketches resolve proxy scores to ~1e-7 relative; a closer near-tie may go
+        # either way in mixed precision (it does not in FP64)
         r = assert_same_or_tied(res["sequence"], ores["sequence"], scores, 1e-6)
         upto = len(res["sequence"]) if r is None else r
         np.testing.assert_allclose(res["marginals"][:upto], ores["marginals"][:upto], rtol=1e-6)
