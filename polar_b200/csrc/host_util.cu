@@ -90,6 +90,13 @@ void timing_collect() {
   g_pending.clear();
 }
 
+void timing_add(int cls, double bytes, float ms) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_cls_count[cls] += 1;
+  g_cls_ms[cls] += ms;
+  g_cls_bytes[cls] += bytes;
+}
+
 }  // namespace polar
 
 extern "C" long long polar_launch_count(void) { return polar::g_launches.load(); }

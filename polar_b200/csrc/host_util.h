@@ -34,5 +34,6 @@ struct TimedLaunch {
 cudaEvent_t timing_event();
 void timing_push(const TimedLaunch& t);
 void timing_collect();  // after a stream sync: fold finished pairs into the totals
+void timing_add(int cls, double bytes, float ms);
 
 }  // namespace polar

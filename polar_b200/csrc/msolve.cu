@@ -399,6 +399,7 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
   add((size_t)ld * 8);                             // 29 chi
   add(4096);                                       // 30 device copy of the parameter block
   add((size_t)p * ld * kNC * 8);                   // 31 composed deferred-update coefficients
+  add((size_t)kMaxHeavyCtas * ld * 8);             // 32 heavy-row d.v partials
   L->total = o;
   L->ld = ld;
   L->vec = choose_vec(precision, ld);
@@ -573,6 +574,8 @@ extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d
     prm.stats = (long long*)(ws + L.off[28]);
     prm.chig = (double*)(ws + L.off[29]);
     prm.cmp = g_solver_mode == 0 ? (double*)(ws + L.off[31]) : nullptr;
+    prm.part_h = (double*)(ws + L.off[32]);
+    prm.nbh = 0;
     prm.timeout_ns = g_timeout_ns;
   };
   int rc;

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <map>
+#include <vector>
 #include <mutex>
 #include <tuple>
 
@@ -101,7 +102,10 @@ __global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolveP
 #define POLAR_SPMM_MINB 2  // resident 512-thread CTAs per SM requested for the SpMM kernel
 #endif
 // CPL: columns per lane (several 16-byte accesses when wider); row group = ld / CPL lanes.
-template <typename T, int CPL, bool W>
+// MODE 1: heavy chunks only (partials of d.v to part_h, no reduction); MODE 2: light rows
+// only, the last CTA reduces both partial arrays.  Two launches give each half its own
+// register budget.
+template <typename T, int CPL, bool W, int MODE>
 __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_constant__ SolvePrm<T> P) {
 
   if (!solve_live(P.ctl, P.stats, P.maxit)) return;
@@ -125,7 +129,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
   // heavy rows, chunked; one warp per chunk: the warp's row groups take interleaved
   // neighbours and combine by shuffles in a fixed pattern (chunk -> warp fixed, so d.v
   // does not depend on which warp finishes the row)
-  {
+  if (MODE == 1) {
     const int wid = blockIdx.x * kWarps + warp;
     const int nw = gridDim.x * kWarps;
     const int grp = lane / rg.G;
@@ -211,6 +215,11 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       __syncwarp();
     }
   }
+  if (MODE == 1) {
+    // heavy-only launch: partial d.v per CTA, reduced by the light launch's last CTA
+    reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part_h + (size_t)blockIdx.x * ld);
+    return;
+  }
   if (g.nsl > 0 && g.sell_s == gpw && !W) {
     // light rows in sliced ELL: a warp takes a slice of gpw degree-sorted rows and reads
     // neighbour k of all its rows with one coalesced load
@@ -232,17 +241,18 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
 #pragma unroll
       for (int v = 0; v < CPL; ++v) acc[v] = A(0);
       const int* sp = g.d_sl_idx + off + grp;
+      constexpr int U = (CPL <= 4) ? 8 : 4;
       int k = 0;
-      for (; k + 4 <= w; k += 4) {
-        int jj[4];
+      for (; k + U <= w; k += U) {
+        int jj[U];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) jj[u] = __ldg(sp + (k + u) * S);
-        T xv[4][CPL];
+        for (int u = 0; u < U; ++u) jj[u] = __ldg(sp + (k + u) * S);
+        T xv[U][CPL];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < U; ++u)
           if (go && jj[u] >= 0) vload<T, CPL>(xv[u], P.d + (size_t)jj[u] * ld + rg.col);
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < U; ++u)
           if (go && jj[u] >= 0)
 #pragma unroll
             for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
@@ -285,6 +295,12 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
   reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
   if (last_cta(P.ctl + C_CNT1)) {
     reduce_partials(P.part, gridDim.x, ld, red, s_col);
+    if (P.nbh > 0) {
+      __shared__ double s_h[kMaxLd];
+      reduce_partials(P.part_h, P.nbh, ld, red, s_h);
+      for (int c = threadIdx.x; c < ld; c += blockDim.x) s_col[c] = s_h[c] + s_col[c];
+      __syncthreads();
+    }
     for (int c = threadIdx.x; c < ld; c += blockDim.x) {
       const int a_on = P.act[c];
       const double a = a_on ? P.rr[c] / s_col[c] : 0.0;
@@ -453,9 +469,12 @@ static int occ_grid(F* fn, int block);
 template <typename T, bool W>
 struct SpmmLaunch {
   template <int CPL>
-  static int grid() { return occ_grid(mk_spmm<T, CPL, W>, kBlock); }
+  static int grid() { return occ_grid(mk_spmm<T, CPL, W, 2>, kBlock); }
   template <int CPL>
-  static void go(int g, const SolvePrm<T>& P, cudaStream_t st) { mk_spmm<T, CPL, W><<<g, kBlock, 0, st>>>(P); }
+  static void go(int g, const SolvePrm<T>& P, cudaStream_t st) {
+    if (P.nbh > 0) mk_spmm<T, CPL, W, 1><<<P.nbh, kBlock, 0, st>>>(P);
+    mk_spmm<T, CPL, W, 2><<<g, kBlock, 0, st>>>(P);
+  }
 };
 
 static int g_spmm_cpl_bytes = 0;  // 0: automatic
@@ -574,7 +593,19 @@ static void timed(int cls, double bytes, cudaStream_t st, F&& launch) {
 }
 
 template <typename T, int VEC, bool W, int E>
-int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
+int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
+  SolvePrm<T> P = P0;
+  // heavy chunks run in their own launch when there are any (one warp per chunk, at most
+  // two CTAs per SM)
+  {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int want = (P.g.nchunks + kWarps - 1) / kWarps;
+    const int cap = 2 * sms;
+    P.nbh = P.g.nchunks > 0 ? (want < cap ? want : cap) : 0;
+    if (P.nbh > kMaxHeavyCtas) P.nbh = kMaxHeavyCtas;
+  }
   (void)dev_prm;
   const double s = sizeof(T), n = P.n, R = P.R, nA = P.nA;
   // algorithmic bytes per launch (unweighted CSR: values implicit, diagonal from indptr)
@@ -595,33 +626,97 @@ int mk_solve(const SolvePrm<T>& P, SolvePrm<T>* dev_prm, cudaStream_t st, MkResu
   timed(KC_INIT, 2.0 * s * n * R + 8.0 * n * R, st, [&] { mk_init<T, VEC><<<g0, kBlock, 0, st>>>(P); });
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error("mk_init", e);
+  // One block = M iterations and one deferred-update pass, captured once per solve as a
+  // CUDA graph (the parameters are fixed for the whole solve) and launched until
+  // convergence.  With kernel timing on, each kernel node is bracketed by event nodes.
+  const bool timing = timing_on();
+  struct GraphTimed {
+    int cls;
+    double bytes;
+    cudaEvent_t a, b;
+  };
+  std::vector<GraphTimed> gt;
+  auto node = [&](cudaStream_t cs, int cls, double bytes, auto&& launch) {
+    if (timing) {
+      GraphTimed t{cls, bytes, nullptr, nullptr};
+      cudaEventCreate(&t.a);
+      cudaEventCreate(&t.b);
+      // inside capture only an external record becomes an event-record node
+      cudaEventRecordWithFlags(t.a, cs, cudaEventRecordExternal);
+      launch(cs);
+      cudaEventRecordWithFlags(t.b, cs, cudaEventRecordExternal);
+      gt.push_back(t);
+    } else {
+      launch(cs);
+    }
+  };
+  cudaStream_t cs;
+  e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return set_cuda_error("capture stream", e);
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(cs);
+    return set_cuda_error("begin capture", e);
+  }
+  for (int k = 0; k < kHist; ++k) {
+    node(cs, KC_SPMM, b_spmm, [&](cudaStream_t x) { spmm_go<T, W>(cpl, g1, P, x); });
+    node(cs, KC_RESID, b_resid, [&](cudaStream_t x) { mk_resid<T, VEC><<<g3, kBlock, 0, x>>>(P, k); });
+    node(cs, KC_DIR, b_dir, [&](cudaStream_t x) { mk_dir<T, VEC><<<g4, kBlock, 0, x>>>(P, k); });
+  }
+  node(cs, KC_FLUSH, b_flush, [&](cudaStream_t x) { mk_flush<T, E><<<g5, kBlock, s5, x>>>(P, 0); });
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(cs, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    for (auto& t : gt) {
+      cudaEventDestroy(t.a);
+      cudaEventDestroy(t.b);
+    }
+  };
+  if (e != cudaSuccess) {
+    cleanup();
+    return set_cuda_error("graph build", e);
+  }
+  const int per_block = (P.nbh > 0 ? 4 : 3) * kHist + 1;
   int ctl[8];
   long long stats[2];
   for (;;) {
-    // M iterations and one deferred-update pass; launches queue ahead of the device
-    for (int k = 0; k < kHist; ++k) {
-      timed(KC_SPMM, b_spmm, st, [&] { spmm_go<T, W>(cpl, g1, P, st); });
-      timed(KC_RESID, b_resid, st, [&] { mk_resid<T, VEC><<<g3, kBlock, 0, st>>>(P, k); });
-      timed(KC_DIR, b_dir, st, [&] { mk_dir<T, VEC><<<g4, kBlock, 0, st>>>(P, k); });
-    }
-    timed(KC_FLUSH, b_flush, st, [&] { mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 0); });
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return set_cuda_error("msolve launch", e);
-    e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
+    e = cudaGraphLaunch(exec, st);
+    count_launch(per_block);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return set_cuda_error("msolve sync", e);
-    if (timing_on()) timing_collect();
+    if (e != cudaSuccess) {
+      cleanup();
+      return set_cuda_error("msolve block", e);
+    }
+    if (timing)
+      for (auto& t : gt) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess)
+          timing_add(t.cls, t.bytes, ms);
+        else
+          cudaGetLastError();
+      }
     if (ctl[C_ERR] != 0 || ctl[C_ANY] == 0) break;
     if (stats[0] >= P.maxit) {
       timed(KC_FLUSH, b_flush, st, [&] { mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 1); });
       e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e != cudaSuccess) return set_cuda_error("msolve sync", e);
+      if (e != cudaSuccess) {
+        cleanup();
+        return set_cuda_error("msolve sync", e);
+      }
       break;
     }
   }
+  if (timing) timing_collect();
+  cleanup();
   out->err = ctl[C_ERR];
   out->capped = ctl[C_ERR] == 0 && ctl[C_ANY] != 0;
   out->iterations = stats[0];

@@ -10,7 +10,8 @@ constexpr int kBlock = 512;
 constexpr int kWarps = kBlock / 32;
 constexpr int kMaxLd = 128;
 constexpr int kHist = 16;  // M: iterations per deferred shifted-update pass
-constexpr int kNC = 2 + 2 * kHist;  // composed coefficients per (pole, column)
+constexpr int kNC = 2 + 2 * kHist;
+constexpr int kMaxHeavyCtas = 1024;  // bound of the heavy-row launch (partials buffer rows)  // composed coefficients per (pole, column)
 #ifndef POLAR_E32
 #define POLAR_E32 2  // active rows per thread in the deferred update, FP32 iterates
 #endif
@@ -38,6 +39,8 @@ template <typename T> struct SolvePrm {
   typename AccOf<T>::type* chunk_part;
   int* hcount;
   double* part;
+  double* part_h;  // per-CTA d.v partials of the heavy-row launch
+  int nbh;         // CTAs of the heavy-row launch (0: none)
   double *rr, *stop, *ap, *bp, *ag, *beg, *chig;
   int *act, *upd;
   double *z, *zp, *hs, *ip, *pn;
