@@ -134,6 +134,15 @@ int polar_spmm_scratch_init(const polar_graph* g, int precision, int R, void* d_
                             polar_stream_t stream);
 int polar_spmm(const polar_graph* g, int precision, int R, double shift, const void* d_X, int ldx,
                void* d_Y, int ldy, void* d_scratch, polar_stream_t stream);
+/* Same apply as polar_spmm with the heavy-row scratch in a fixed 8 MiB device array inside
+ * the library, so the call allocates nothing.  No counterpart in the reference: it serves
+ * callers that may not allocate device memory when they apply the operator.  Returns
+ * POLAR_ERR_WORKSPACE when polar_spmm_scratch_bytes(g, precision, R) exceeds 8 MiB.  The
+ * first call on each device resolves the array's address (cudaGetSymbolAddress) and should
+ * come before any stream capture.  All calls on a device share the array: calls that
+ * overlap in time race and must be serialised by the caller. */
+int polar_spmm_noalloc(const polar_graph* g, int precision, int R, double shift, const void* d_X, int ldx,
+                       void* d_Y, int ldy, polar_stream_t stream);
 
 /* ---- multi-shift CG (polar_gpu.py:88-133) ----
  * Solves (M + tau_j I) U_j = W for all p poles and R columns in ONE persistent

@@ -76,6 +76,7 @@ SIGNATURES = {
     "polar_spmm_scratch_bytes": (_S, [_GP, _I, _I]),
     "polar_spmm_scratch_init": (_I, [_GP, _I, _I, _P, _P]),
     "polar_spmm": (_I, [_GP, _I, _I, _D, _P, _I, _P, _I, _P, _P]),
+    "polar_spmm_noalloc": (_I, [_GP, _I, _I, _D, _P, _I, _P, _I, _P]),
     "polar_msolve_workspace_bytes": (_S, [_GP, _I, _I, _I, _I]),
     "polar_msolve": (_I, [_GP, _I, _P, _I, _I, _P, _I, _P, _P, _I, _D, _I64, _I, _P, _I, _I, _P, _P, _P, _S, _P]),
     "polar_msolve_finish": (_I, [_P, _P, ctypes.POINTER(MsolveInfo)]),
