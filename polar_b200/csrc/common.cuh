@@ -70,6 +70,14 @@ POLAR_D void vstore(T* p, const T (&in)[V]) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Programmatic dependent launch (sm_90+).  A kernel launched with programmatic stream
+// serialization may start while its predecessor is still running; pdl_wait blocks until
+// the predecessor grid has completed and its memory is visible (a no-op for an ordinary
+// launch).  pdl_launch lets the successor be scheduled once every CTA of this grid has
+// called it, so the successor's CTAs take SM slots as this grid's CTAs retire.
+POLAR_D void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+POLAR_D void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 POLAR_D uint64_t globaltimer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

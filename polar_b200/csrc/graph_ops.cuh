@@ -151,7 +151,8 @@ POLAR_D double added_terms(const polar_graph& g, const RowGroup& rg, int i, cons
 }
 
 // Finishes row i from its own entries xi (already loaded): y = (diag + shift) x_i - acc.
-template <typename T, int VEC>
+// ADD = false leaves out the added edges (the caller applies them afterwards).
+template <typename T, int VEC, bool ADD = true>
 POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int deg, double shift, const T* X,
                             int ld, typename AccOf<T>::type (&acc)[VEC], T* Y, int ldy, const T (&xi)[VEC],
                             T (&yi)[VEC], bool store = true) {
@@ -161,7 +162,7 @@ POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int
     for (int v = 0; v < VEC; ++v) yi[v] = T(0);
     return;
   }
-  const double wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
+  const double wadd = ADD ? added_terms<T, VEC>(g, rg, i, X, ld, acc) : 0.0;
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
 #pragma unroll
   for (int v = 0; v < VEC; ++v) yi[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
@@ -169,7 +170,7 @@ POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int
 }
 
 // Finishes row i: y = (diag + shift) x_i - acc.  Returns x_i in xi (for d^T v).
-template <typename T, int VEC>
+template <typename T, int VEC, bool ADD = true>
 POLAR_D void finish_row(const polar_graph& g, const RowGroup& rg, int i, int deg, double shift,
                         const T* X, int ld, typename AccOf<T>::type (&acc)[VEC], T* Y,
                         int ldy, T (&xi)[VEC], T (&yi)[VEC], bool store = true) {
@@ -179,7 +180,7 @@ POLAR_D void finish_row(const polar_graph& g, const RowGroup& rg, int i, int deg
     for (int v = 0; v < VEC; ++v) xi[v] = yi[v] = T(0);
     return;
   }
-  const double wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
+  const double wadd = ADD ? added_terms<T, VEC>(g, rg, i, X, ld, acc) : 0.0;
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
   vload<T, VEC>(xi, X + (size_t)i * ld + rg.col);
 #pragma unroll

@@ -16,6 +16,7 @@
 // deterministic (fixed grids, fixed summation order).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <map>
 #include <vector>
 #include <mutex>
@@ -97,17 +98,74 @@ __global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolveP
   }
 }
 
+// ---- edges added by the greedy (Op.add): v += sum_S w b b^T d, d.v += d^T (that) ------------
+// Run by the SpMM's last CTA after every row of v is final.  Thread item = (added-edge
+// row, column); each row's change is its own term w (d_r - d_k) summed over its added
+// neighbours in list order, and the d.v correction x_r (v_new - v_old) is summed per column
+// over the rows in a fixed order in `tmp` (shared, kWarps * kMaxLd doubles).
+template <typename T>
+POLAR_D void apply_added_edges(const SolvePrm<T>& P, double* tmp, double* s_col) {
+  const polar_graph& g = P.g;
+  const int ld = P.ld;
+  const int tile = (kWarps * kMaxLd) / ld;
+  double colsum = 0.0;
+  for (int r0 = 0; r0 < g.nx; r0 += tile) {
+    const int nr = min(tile, g.nx - r0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < nr * ld; q += blockDim.x) {
+      const int rr = q / ld, c = q - rr * ld;
+      const int ix = r0 + rr;
+      const int r = __ldg(g.d_xrow + ix);
+      const int b = __ldg(g.d_xoff + ix), e = __ldg(g.d_xoff + ix + 1);
+      const double dr = (double)P.d[(size_t)r * ld + c];
+      double delta = 0.0;
+      for (int k = b; k < e; ++k) {
+        const double w = g.d_xwt ? __ldg(g.d_xwt + k) : 1.0;
+        delta += w * (dr - (double)P.d[(size_t)__ldg(g.d_xnbr + k) * ld + c]);
+      }
+      T* vp = P.v + (size_t)r * ld + c;
+      const T vold = *vp;
+      const T vnew = (T)((double)vold + delta);
+      *vp = vnew;
+      tmp[rr * ld + c] = dr * ((double)vnew - (double)vold);
+    }
+    __syncthreads();
+    if (threadIdx.x < ld)
+      for (int rr = 0; rr < nr; ++rr) colsum += tmp[rr * ld + threadIdx.x];
+  }
+  __syncthreads();
+  if (threadIdx.x < ld) s_col[threadIdx.x] += colsum;
+  __syncthreads();
+}
+
 // ---- v = (M + tau_0 I) d and d.v -------------------------------------------------------
 #ifndef POLAR_SPMM_MINB
 #define POLAR_SPMM_MINB 2  // resident 512-thread CTAs per SM requested for the SpMM kernel
 #endif
+// Bytes of gathered rows in flight per lane: the gather batch is this many bytes over the
+// lane's share of a row (at least one neighbour).  Larger batches spill at 64 registers.
+#ifndef POLAR_STREAM_U
+#define POLAR_STREAM_U 4  // row items in flight per thread in the d update
+#endif
+#ifndef POLAR_RESID_U
+#define POLAR_RESID_U 2   // same for the r update (more spills at 64 registers)
+#endif
+#ifndef POLAR_HEAVY_BYTES
+#define POLAR_HEAVY_BYTES 64
+#endif
+#ifndef POLAR_SELL_BYTES
+#define POLAR_SELL_BYTES 64
+#endif
 // CPL: columns per lane (several 16-byte accesses when wider); row group = ld / CPL lanes.
 // MODE 1: heavy chunks only (partials of d.v to part_h, no reduction); MODE 2: light rows
-// only, the last CTA reduces both partial arrays.  Two launches give each half its own
-// register budget.
+// by row groups, MODE 3: light rows from the sliced-ELL copy (unweighted graphs); in both
+// the last CTA reduces the partial arrays.  Separate instantiations give each path its
+// own register budget.
 template <typename T, int CPL, bool W, int MODE>
 __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_constant__ SolvePrm<T> P) {
 
+  pdl_wait();
+  pdl_launch();
   if (!solve_live(P.ctl, P.stats, P.maxit)) return;
   using A = typename AccOf<T>::type;
   __shared__ double red[kWarps * kMaxLd];
@@ -123,13 +181,19 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
   bool on = false;
 #pragma unroll
   for (int v = 0; v < CPL; ++v) on |= P.act[rg.col + v] != 0;
-  double dacc[CPL];
-#pragma unroll
-  for (int v = 0; v < CPL; ++v) dacc[v] = 0.0;
-  // heavy rows, chunked; one warp per chunk: the warp's row groups take interleaved
-  // neighbours and combine by shuffles in a fixed pattern (chunk -> warp fixed, so d.v
-  // does not depend on which warp finishes the row)
+  // heavy rows, in chunks of at most kChunkMax neighbours, one warp per chunk.  The warp
+  // stages the chunk's indices in shared memory with one coalesced pass; row group grp
+  // then takes neighbours grp, grp + gpw, ... in batches of U independent gathers, and the
+  // groups combine by shuffles in a fixed pattern.  A row held in one chunk is finished by
+  // the warp; longer rows leave per-chunk partials that the last chunk to arrive sums in
+  // chunk order, so neither v nor d.v depends on scheduling.
   if (MODE == 1) {
+    constexpr int LB = CPL * (int)sizeof(T);
+    constexpr int U = (POLAR_HEAVY_BYTES / LB) > 1 ? (POLAR_HEAVY_BYTES / LB) : 1;
+    __shared__ int s_idx[kWarps][kChunkMax];
+    double dacc[CPL];
+#pragma unroll
+    for (int v = 0; v < CPL; ++v) dacc[v] = 0.0;
     const int wid = blockIdx.x * kWarps + warp;
     const int nw = gridDim.x * kWarps;
     const int grp = lane / rg.G;
@@ -138,56 +202,61 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
       const int i = __ldg(g.d_hrow + h);
       const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
+      const bool single = (c1 - c0) == 1;
+      T xi[CPL];
+      if (on && grp == 0) vload<T, CPL>(xi, P.d + (size_t)i * ld + rg.col);
+      const int cnt = hi - lo;
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < kChunkMax / 32; ++q) {
+        const int k = 32 * q + lane;
+        if (k < cnt) s_idx[warp][k] = __ldg(g.d_indices + lo + k);
+      }
+      __syncwarp();
       A acc[CPL];
 #pragma unroll
       for (int v = 0; v < CPL; ++v) acc[v] = A(0);
-      for (int k0 = lo; k0 < hi; k0 += 32) {
-        const int k = k0 + lane;
-        int j = 0;
-        A w = A(1);
-        if (k < hi) {
-          j = __ldg(g.d_indices + k);
-          if (W) w = (A)__ldg(g.d_wts + k);
-        }
-        const int cnt = min(32, hi - k0);
-        for (int t0 = 0; t0 < cnt; t0 += 4 * gpw) {
-          T xv[4][CPL];
-          A ww[4];
-          bool okk[4];
+      const int nu = cnt > grp ? (cnt - grp + gpw - 1) / gpw : 0;
+      const int numax = (cnt + gpw - 1) / gpw;
+      for (int u0 = 0; u0 < numax; u0 += U) {
+        T xv[U][CPL];
+        A wv[U];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int t = t0 + u * gpw + grp;
-            const int jt = __shfl_sync(0xffffffffu, j, t & 31);
-            ww[u] = W ? __shfl_sync(0xffffffffu, w, t & 31) : A(1);
-            okk[u] = t < cnt && on;
-            if (okk[u]) vload<T, CPL>(xv[u], P.d + (size_t)jt * ld + rg.col);
+        for (int uu = 0; uu < U; ++uu)
+          if (on && u0 + uu < nu) {
+            const int t = grp + gpw * (u0 + uu);
+            vload<T, CPL>(xv[uu], P.d + (size_t)s_idx[warp][t] * ld + rg.col);
+            wv[uu] = W ? (A)__ldg(g.d_wts + lo + t) : A(1);
           }
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
-            if (okk[u])
+        for (int uu = 0; uu < U; ++uu)
+          if (on && u0 + uu < nu) {
 #pragma unroll
-              for (int v = 0; v < CPL; ++v)
-                acc[v] = W ? fma(ww[u], (A)xv[u][v], acc[v]) : acc[v] + (A)xv[u][v];
-        }
+            for (int v = 0; v < CPL; ++v) acc[v] = W ? fma(wv[uu], (A)xv[uu][v], acc[v]) : acc[v] + (A)xv[uu][v];
+          }
       }
       for (int o = rg.G; o < 32; o <<= 1)
 #pragma unroll
         for (int v = 0; v < CPL; ++v) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
-      T xi[CPL];
+      if (single) {
+        if (grp == 0) {
+          T yi[CPL];
+          finish_row_pre<T, CPL, false>(g, rg, i, cnt, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
+          if (on)
+#pragma unroll
+            for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+        }
+        continue;
+      }
       if (on && grp == 0) {
         vstore<A, CPL>(P.chunk_part + (size_t)ch * ld + rg.col, acc);
-        vload<T, CPL>(xi, P.d + (size_t)i * ld + rg.col);
 #pragma unroll
         for (int v = 0; v < CPL; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
         if (ch == c0) {
-          A ex[CPL];
-#pragma unroll
-          for (int v = 0; v < CPL; ++v) ex[v] = A(0);
-          const double wadd = added_terms<T, CPL>(g, rg, i, P.d, ld, ex);
           const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-          const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
+          const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + shift;
 #pragma unroll
-          for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v] - (double)ex[v]);
+          for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v]);
         }
       }
       __threadfence();
@@ -209,90 +278,122 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
           }
         const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
         T xf[CPL], yi[CPL];
-        finish_row<T, CPL>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
+        finish_row<T, CPL, false>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
         if (lane == 0) P.hcount[h] = 0;
       }
       __syncwarp();
     }
-  }
-  if (MODE == 1) {
     // heavy-only launch: partial d.v per CTA, reduced by the light launch's last CTA
     reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part_h + (size_t)blockIdx.x * ld);
     return;
   }
-  if (g.nsl > 0 && g.sell_s == gpw && !W) {
+  if (MODE == 3) {
     // light rows in sliced ELL: a warp takes a slice of gpw degree-sorted rows and reads
-    // neighbour k of all its rows with one coalesced load
+    // neighbour k of all its rows with one coalesced load.  Neighbours go in batches of U
+    // predicated gathers (short rows issue all theirs at once), the next slice's
+    // descriptors are fetched while this one is gathered, and a row's degree is the count
+    // of its valid entries (the slice holds exactly the CSR neighbours).  The row's own
+    // entries are read after its gathers.  d.v leaves the registers: after each slice the
+    // products x_i y_i are summed over the warp's rows per column in FP64 (fixed xor
+    // pattern) and added to the warp's row of `red`.
+    constexpr int LB = CPL * (int)sizeof(T);
+    constexpr int U = (POLAR_SELL_BYTES / LB) > 1 ? (POLAR_SELL_BYTES / LB) : 1;
+    constexpr int DC = CPL < 4 ? CPL : 4;  // columns per FP64 reduction pass
     const int wid = blockIdx.x * kWarps + warp;
     const int nw = gridDim.x * kWarps;
     const int grp = lane / rg.G;
     const int S = gpw;
+    double* wred = red + warp * ld;
+    for (int c = lane; c < ld; c += 32) wred[c] = 0.0;
+    __syncwarp();
+    int off_n = 0, end_n = 0, row_n = -1;
+    if (wid < g.nsl) {
+      off_n = __ldg(g.d_sl_off + wid);
+      end_n = __ldg(g.d_sl_off + wid + 1);
+      row_n = __ldg(g.d_sl_rows + (size_t)wid * S + grp);
+    }
     for (int sl = wid; sl < g.nsl; sl += nw) {
-      const int off = __ldg(g.d_sl_off + sl);
-      const int w = (__ldg(g.d_sl_off + sl + 1) - off) / S;
-      const int row = __ldg(g.d_sl_rows + sl * S + grp);
+      const int off = off_n, w = (end_n - off_n) / S, row = row_n;
+      const int sn = sl + nw;
+      if (sn < g.nsl) {
+        off_n = __ldg(g.d_sl_off + sn);
+        end_n = __ldg(g.d_sl_off + sn + 1);
+        row_n = __ldg(g.d_sl_rows + (size_t)sn * S + grp);
+      }
       const bool valid = row >= 0;
       const bool go = valid && on;
-      T xi[CPL], yi[CPL];
-      int deg = 0;
-      if (valid) deg = __ldg(g.d_indptr + row + 1) - __ldg(g.d_indptr + row);
-      if (go) vload<T, CPL>(xi, P.d + (size_t)row * ld + rg.col);
       A acc[CPL];
 #pragma unroll
       for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+      int deg = 0;
       const int* sp = g.d_sl_idx + off + grp;
-      constexpr int U = (CPL <= 4) ? 8 : 4;
-      int k = 0;
-      for (; k + U <= w; k += U) {
+      for (int k = 0; k < w; k += U) {
         int jj[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) jj[u] = __ldg(sp + (k + u) * S);
+        for (int u = 0; u < U; ++u) jj[u] = (k + u < w) ? __ldg(sp + (size_t)(k + u) * S) : -1;
         T xv[U][CPL];
 #pragma unroll
         for (int u = 0; u < U; ++u)
           if (go && jj[u] >= 0) vload<T, CPL>(xv[u], P.d + (size_t)jj[u] * ld + rg.col);
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          if (go && jj[u] >= 0)
+          if (jj[u] >= 0) {
+            ++deg;
+            if (go)
 #pragma unroll
-            for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
+              for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
+          }
       }
-      for (; k < w; ++k) {
-        const int jj = __ldg(sp + k * S);
-        if (go && jj >= 0) {
-          T xv[CPL];
-          vload<T, CPL>(xv, P.d + (size_t)jj * ld + rg.col);
+      // y_i = (deg + sigma + added + shift) x_i - acc, formed in place in acc
+      T xi[CPL];
+      if (go) {
+        vload<T, CPL>(xi, P.d + (size_t)row * ld + rg.col);
+        const double dg = (double)deg + g.sigma + shift;
+        T yv[CPL];
 #pragma unroll
-          for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[v];
-        }
+        for (int v = 0; v < CPL; ++v) yv[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
+        vstore<T, CPL>(P.v + (size_t)row * ld + rg.col, yv);
+#pragma unroll
+        for (int v = 0; v < CPL; ++v) acc[v] = (A)yv[v];
       }
-      if (valid) {
-        finish_row_pre<T, CPL>(g, rg, row, deg, shift, P.d, ld, acc, P.v, ld, xi, yi, go);
-        if (go)
 #pragma unroll
-          for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+      for (int v0 = 0; v0 < CPL; v0 += DC) {
+        double pr[DC];
+#pragma unroll
+        for (int v = 0; v < DC; ++v) pr[v] = go ? (double)xi[v0 + v] * (double)acc[v0 + v] : 0.0;
+        for (int o = rg.G; o < 32; o <<= 1)
+#pragma unroll
+          for (int v = 0; v < DC; ++v) pr[v] += __shfl_xor_sync(0xffffffffu, pr[v], o);
+        if (lane < rg.G)
+#pragma unroll
+          for (int v = 0; v < DC; ++v) wred[rg.col + v0 + v] += pr[v];
       }
     }
+    reduce_red_to_part(red, ld, P.part + (size_t)blockIdx.x * ld);
   } else {
-    // light rows, one row group per row; the row's own entries are loaded with its indices
+    // MODE 2: light rows, one row group per row; the row's own entries are loaded with its
+    // indices
+    double dl[CPL];
+#pragma unroll
+    for (int v = 0; v < CPL; ++v) dl[v] = 0.0;
     for (int i = gid; i < g.n; i += GT) {
       const int lo = __ldg(g.d_indptr + i), hi = __ldg(g.d_indptr + i + 1);
       if (hi - lo > g.heavy_thresh) continue;
       T xi[CPL], yi[CPL];
       if (on) vload<T, CPL>(xi, P.d + (size_t)i * ld + rg.col);
       A acc[CPL];
-  #pragma unroll
+#pragma unroll
       for (int v = 0; v < CPL; ++v) acc[v] = A(0);
       gather_rows<T, CPL, W>(g, rg, lo, hi, P.d, ld, acc, on);
-      finish_row_pre<T, CPL>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
+      finish_row_pre<T, CPL, false>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
       if (!on)
-  #pragma unroll
+#pragma unroll
         for (int v = 0; v < CPL; ++v) xi[v] = T(0);
-  #pragma unroll
-      for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
+#pragma unroll
+      for (int v = 0; v < CPL; ++v) dl[v] += (double)xi[v] * (double)yi[v];
     }
+    reduce_cols_to_part<CPL>(dl, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
   }
-  reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
   if (last_cta(P.ctl + C_CNT1)) {
     reduce_partials(P.part, gridDim.x, ld, red, s_col);
     if (P.nbh > 0) {
@@ -301,6 +402,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       for (int c = threadIdx.x; c < ld; c += blockDim.x) s_col[c] = s_h[c] + s_col[c];
       __syncthreads();
     }
+    if (g.nx > 0) apply_added_edges(P, red, s_col);
     for (int c = threadIdx.x; c < ld; c += blockDim.x) {
       const int a_on = P.act[c];
       const double a = a_on ? P.rr[c] / s_col[c] : 0.0;
@@ -314,6 +416,8 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ SolvePrm<T> P, int slot) {
 
+  pdl_wait();
+  pdl_launch();
   if (!solve_live(P.ctl, P.stats, P.maxit)) return;
   __shared__ double red[kWarps * kMaxLd];
   __shared__ double s_col[kMaxLd];
@@ -334,10 +438,11 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
   }
   if (any_on) {
     T* hslot = P.hist + (size_t)slot * nA * ld;
-    constexpr int U = 2;
+    constexpr int U = POLAR_RESID_U;
     for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
       T rv[U][VEC], vv[U][VEC];
       long long ii[U];
+      int ai[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const long long e = e0 + u * nth;
@@ -345,6 +450,7 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
         if (ii[u] >= 0) {
           vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
           vload<T, VEC>(vv[u], P.v + (size_t)ii[u] * ld + rg.col);
+          ai[u] = __ldg(P.active_pos + ii[u]);
         }
       }
 #pragma unroll
@@ -356,8 +462,7 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
           racc[v] += (double)rv[u][v] * (double)rv[u][v];
         }
         vstore<T, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
-        const int ai = __ldg(P.active_pos + ii[u]);
-        if (ai >= 0) vstore<T, VEC>(hslot + (size_t)ai * ld + rg.col, rv[u]);
+        if (ai[u] >= 0) vstore<T, VEC>(hslot + (size_t)ai[u] * ld + rg.col, rv[u]);
       }
     }
   }
@@ -377,6 +482,8 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
 template <typename T, int VEC>
 __global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ SolvePrm<T> P, int slot) {
 
+  pdl_wait();
+  pdl_launch();
   if (ld_volatile_i32(P.ctl + C_RAN) == 0) return;
   const int ld = P.ld;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -397,7 +504,7 @@ __global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ Solv
       any_on |= on[v];
     }
     if (any_on) {
-      constexpr int U = 2;
+      constexpr int U = POLAR_STREAM_U;
       for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
         T rv[U][VEC], dv[U][VEC];
         long long ii[U];
@@ -434,6 +541,8 @@ template <typename T, int E>
 __global__ void __launch_bounds__(kBlock, 2) mk_flush(const __grid_constant__ SolvePrm<T> P, int force_final) {
   extern __shared__ __align__(16) unsigned char flush_sm[];
 
+  pdl_wait();
+  pdl_launch();
   const int nsteps = ld_volatile_i32(P.ctl + C_NSTEPS);
   const bool first = ld_volatile_i32(P.ctl + C_FIRST) != 0;
   const bool done = ld_volatile_i32(P.ctl + C_ANY) == 0 || ld_volatile_i32(P.ctl + C_ERR) != 0;
@@ -465,6 +574,31 @@ __global__ void __launch_bounds__(kBlock, 2) mk_flush(const __grid_constant__ So
 template <typename F>
 static int occ_grid(F* fn, int block);
 
+// Kernel launch with programmatic stream serialization (on unless POLAR_PDL=0): inside the
+// captured iteration block each kernel's launch overlaps its predecessor's tail.
+static bool pdl_on() {
+  static const bool on = [] {
+    const char* e = getenv("POLAR_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_on() ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // SpMM launch for a runtime choice of columns per lane.
 template <typename T, bool W>
 struct SpmmLaunch {
@@ -472,8 +606,12 @@ struct SpmmLaunch {
   static int grid() { return occ_grid(mk_spmm<T, CPL, W, 2>, kBlock); }
   template <int CPL>
   static void go(int g, const SolvePrm<T>& P, cudaStream_t st) {
-    if (P.nbh > 0) mk_spmm<T, CPL, W, 1><<<P.nbh, kBlock, 0, st>>>(P);
-    mk_spmm<T, CPL, W, 2><<<g, kBlock, 0, st>>>(P);
+    if (P.nbh > 0) launch_k(mk_spmm<T, CPL, W, 1>, P.nbh, kBlock, 0, st, P);
+    const int gpw = 32 / (P.ld / CPL);
+    if (!W && P.g.nsl > 0 && P.g.sell_s == gpw)
+      launch_k(mk_spmm<T, CPL, W, 3>, g, kBlock, 0, st, P);
+    else
+      launch_k(mk_spmm<T, CPL, W, 2>, g, kBlock, 0, st, P);
   }
 };
 
@@ -660,10 +798,10 @@ int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkRes
   }
   for (int k = 0; k < kHist; ++k) {
     node(cs, KC_SPMM, b_spmm, [&](cudaStream_t x) { spmm_go<T, W>(cpl, g1, P, x); });
-    node(cs, KC_RESID, b_resid, [&](cudaStream_t x) { mk_resid<T, VEC><<<g3, kBlock, 0, x>>>(P, k); });
-    node(cs, KC_DIR, b_dir, [&](cudaStream_t x) { mk_dir<T, VEC><<<g4, kBlock, 0, x>>>(P, k); });
+    node(cs, KC_RESID, b_resid, [&](cudaStream_t x) { launch_k(mk_resid<T, VEC>, g3, kBlock, 0, x, P, k); });
+    node(cs, KC_DIR, b_dir, [&](cudaStream_t x) { launch_k(mk_dir<T, VEC>, g4, kBlock, 0, x, P, k); });
   }
-  node(cs, KC_FLUSH, b_flush, [&](cudaStream_t x) { mk_flush<T, E><<<g5, kBlock, s5, x>>>(P, 0); });
+  node(cs, KC_FLUSH, b_flush, [&](cudaStream_t x) { launch_k(mk_flush<T, E>, g5, kBlock, s5, x, P, 0); });
   cudaGraph_t graph = nullptr;
   e = cudaStreamEndCapture(cs, &graph);
   cudaGraphExec_t exec = nullptr;

@@ -166,7 +166,7 @@ class Graph:
     def _split_heavy(self, thresh):
         """Default partition (threshold `thresh`) plus a cache of partitions for other
         thresholds: rows with more than `thresh` neighbours are cut into chunks of at most
-        CHUNK, combined in chunk order by the kernels."""
+        CHUNK (the kernels' kChunkMax), combined in chunk order by the kernels."""
         self.heavy_thresh = max(1, thresh)
         self._heavy = {}
         hv = self._heavy_parts(self.heavy_thresh)
@@ -178,7 +178,7 @@ class Graph:
     def _heavy_parts(self, thresh):
         if thresh in self._heavy:
             return self._heavy[thresh]
-        ch = min(self.CHUNK, max(1, thresh)) if thresh < self.CHUNK else self.CHUNK
+        ch = self.CHUNK
         degs = np.diff(self._indptr_h.astype(np.int64))
         hrow = np.flatnonzero(degs > thresh).astype(np.int32)
         nch = -(-degs[hrow] // ch) if len(hrow) else np.zeros(0, np.int64)

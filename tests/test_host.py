@@ -121,7 +121,8 @@ def test_graph_host_structures_and_heavy_split():
         segs = list(zip(lo[off[h]:off[h + 1]], hi[off[h]:off[h + 1]]))
         assert segs[0][0] == G._indptr_h[r] and segs[-1][1] == G._indptr_h[r + 1]
         assert all(b0 == a1 for (_, a1), (b0, _) in zip(segs[:-1], segs[1:]))
-        assert all(b - a <= 16 for a, b in segs)
+        assert all(0 < b - a <= G.CHUNK for a, b in segs)
+        assert len(segs) == -(-(G._indptr_h[r + 1] - G._indptr_h[r]) // G.CHUNK)
         assert np.all(row[off[h]:off[h + 1]] == h)
     s = G.struct()
     assert s.nheavy == G.nheavy and s.nchunks == G.nchunks and s.d_wts is None
