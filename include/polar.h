@@ -116,9 +116,10 @@ int polar_version(void);
  * polar_launch_count: kernels launched by this library so far (all entry points).
  * polar_set_kernel_timing(1) resets and enables per-class device timing of the
  * solver's kernels (CUDA events around each launch); polar_kernel_timing returns, for
- * class 0 SpMM, 1 residual update, 2 direction/pole update, 3 deferred update, 4 init,
- * the number of timed launches, their summed device time (ms) and summed algorithmic
- * bytes (SpMM: 4(n+1) + 4 nnz + 2 s n R; residual: 3 s n R + s nA R; direction:
+ * class 0 SpMM (light rows), 6 SpMM heavy-row launch, 1 residual update,
+ * 2 direction/pole update, 3 deferred update, 4 init, the number of timed launches, their
+ * summed device time (ms) and summed algorithmic bytes (SpMM, both launches together,
+ * counted on class 0: 4(n+1) + 4 nnz + 2 s n R; residual: 3 s n R + s nA R; direction:
  * 3 s n R; deferred update: (4p + M) s nA R). */
 long long polar_launch_count(void);
 void polar_set_kernel_timing(int on);

@@ -23,7 +23,7 @@ bool lookup_solve(void* ws, SolveRecord* out);
 // Kernel instrumentation: every launch of a libpolar kernel is counted; with timing on,
 // the solver's kernels are bracketed by CUDA events and their device time and
 // algorithmic bytes are accumulated per class.
-enum KernelClass { KC_SPMM = 0, KC_RESID, KC_DIR, KC_FLUSH, KC_INIT, KC_OTHER, KC_COUNT };
+enum KernelClass { KC_SPMM = 0, KC_RESID, KC_DIR, KC_FLUSH, KC_INIT, KC_OTHER, KC_HEAVY, KC_COUNT };
 void count_launch(int n = 1);
 bool timing_on();
 struct TimedLaunch {

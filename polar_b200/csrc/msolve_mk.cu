@@ -158,9 +158,10 @@ POLAR_D void apply_added_edges(const SolvePrm<T>& P, double* tmp, double* s_col)
 #endif
 // CPL: columns per lane (several 16-byte accesses when wider); row group = ld / CPL lanes.
 // MODE 1: heavy chunks only (partials of d.v to part_h, no reduction); MODE 2: light rows
-// by row groups, MODE 3: light rows from the sliced-ELL copy (unweighted graphs); in both
-// the last CTA reduces the partial arrays.  Separate instantiations give each path its
-// own register budget.
+// by row groups (after a MODE 1 launch); MODE 3 (unweighted graphs with a sliced-ELL copy):
+// heavy chunks and then the light rows' slices in one launch.  In modes 2 and 3 the last
+// CTA reduces the partial arrays.  Separate instantiations give each path its own
+// register budget.
 template <typename T, int CPL, bool W, int MODE>
 __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_constant__ SolvePrm<T> P) {
 
@@ -187,7 +188,13 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
   // groups combine by shuffles in a fixed pattern.  A row held in one chunk is finished by
   // the warp; longer rows leave per-chunk partials that the last chunk to arrive sums in
   // chunk order, so neither v nor d.v depends on scheduling.
-  if (MODE == 1) {
+  // MODE 3 accumulates d.v in the warp's row of `red` (heavy chunks first, then slices)
+  double* wred = red + warp * ld;
+  if (MODE == 3) {
+    for (int c = lane; c < ld; c += 32) wred[c] = 0.0;
+    __syncwarp();
+  }
+  if (MODE == 1 || MODE == 3) {
     constexpr int LB = CPL * (int)sizeof(T);
     constexpr int U = (POLAR_HEAVY_BYTES / LB) > 1 ? (POLAR_HEAVY_BYTES / LB) : 1;
     __shared__ int s_idx[kWarps][kChunkMax];
@@ -283,9 +290,19 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       }
       __syncwarp();
     }
-    // heavy-only launch: partial d.v per CTA, reduced by the light launch's last CTA
-    reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part_h + (size_t)blockIdx.x * ld);
-    return;
+    if (MODE == 1) {
+      // heavy-only launch: partial d.v per CTA, reduced by the light launch's last CTA
+      reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part_h + (size_t)blockIdx.x * ld);
+      return;
+    }
+    // MODE 3: fold the heavy rows' d.v into the warp's row (fixed xor pattern)
+    for (int o = rg.G; o < 32; o <<= 1)
+#pragma unroll
+      for (int v = 0; v < CPL; ++v) dacc[v] += __shfl_xor_sync(0xffffffffu, dacc[v], o);
+    if (lane < rg.G)
+#pragma unroll
+      for (int v = 0; v < CPL; ++v) wred[rg.col + v] += dacc[v];
+    __syncwarp();
   }
   if (MODE == 3) {
     // light rows in sliced ELL: a warp takes a slice of gpw degree-sorted rows and reads
@@ -303,9 +320,6 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
     const int nw = gridDim.x * kWarps;
     const int grp = lane / rg.G;
     const int S = gpw;
-    double* wred = red + warp * ld;
-    for (int c = lane; c < ld; c += 32) wred[c] = 0.0;
-    __syncwarp();
     int off_n = 0, end_n = 0, row_n = -1;
     if (wid < g.nsl) {
       off_n = __ldg(g.d_sl_off + wid);
@@ -599,16 +613,26 @@ static void launch_k(void (*k)(KArgs...), int grid, int block, size_t smem, cuda
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
+// True when the SpMM runs as one sliced-ELL launch (MODE 3).
+template <typename T, bool W>
+static bool spmm_merged(int cpl, const SolvePrm<T>& P) {
+  const int gpw = 32 / (P.ld / cpl);
+  return !W && P.g.nsl > 0 && P.g.sell_s == gpw;
+}
+
 // SpMM launch for a runtime choice of columns per lane.
 template <typename T, bool W>
 struct SpmmLaunch {
   template <int CPL>
   static int grid() { return occ_grid(mk_spmm<T, CPL, W, 2>, kBlock); }
+  // part 1: heavy-row launch, part 2: light-row launch
   template <int CPL>
-  static void go(int g, const SolvePrm<T>& P, cudaStream_t st) {
-    if (P.nbh > 0) launch_k(mk_spmm<T, CPL, W, 1>, P.nbh, kBlock, 0, st, P);
-    const int gpw = 32 / (P.ld / CPL);
-    if (!W && P.g.nsl > 0 && P.g.sell_s == gpw)
+  static void go(int part, int g, const SolvePrm<T>& P, cudaStream_t st) {
+    if (part == 1) {
+      if (P.nbh > 0) launch_k(mk_spmm<T, CPL, W, 1>, P.nbh, kBlock, 0, st, P);
+      return;
+    }
+    if (spmm_merged<T, W>(CPL, P))
       launch_k(mk_spmm<T, CPL, W, 3>, g, kBlock, 0, st, P);
     else
       launch_k(mk_spmm<T, CPL, W, 2>, g, kBlock, 0, st, P);
@@ -654,16 +678,16 @@ static int spmm_grid(int cpl) {
 }
 
 template <typename T, bool W>
-static void spmm_go(int cpl, int g, const SolvePrm<T>& P, cudaStream_t st) {
+static void spmm_go(int part, int cpl, int g, const SolvePrm<T>& P, cudaStream_t st) {
   using L = SpmmLaunch<T, W>;
   switch (cpl) {
-    case 1: L::template go<1>(g, P, st); break;
-    case 2: L::template go<2>(g, P, st); break;
-    case 4: L::template go<4>(g, P, st); break;
-    case 8: L::template go<8>(g, P, st); break;
+    case 1: L::template go<1>(part, g, P, st); break;
+    case 2: L::template go<2>(part, g, P, st); break;
+    case 4: L::template go<4>(part, g, P, st); break;
+    case 8: L::template go<8>(part, g, P, st); break;
     default:
-      if (sizeof(T) == 4) L::template go<16>(g, P, st);
-      else L::template go<8>(g, P, st);
+      if (sizeof(T) == 4) L::template go<16>(part, g, P, st);
+      else L::template go<8>(part, g, P, st);
   }
 }
 
@@ -734,7 +758,7 @@ template <typename T, int VEC, bool W, int E>
 int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
   SolvePrm<T> P = P0;
   // heavy chunks run in their own launch when there are any (one warp per chunk, at most
-  // two CTAs per SM)
+  // two CTAs per SM), except on the sliced-ELL path, whose launch takes them first
   {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -753,6 +777,7 @@ int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkRes
   const double b_flush = (4.0 * P.p + kHist) * s * nA * R;
   const int g0 = occ_grid(mk_init<T, VEC>, kBlock);
   const int cpl = spmm_cpl<T>(P.ld, VEC);
+  if (spmm_merged<T, W>(cpl, P)) P.nbh = 0;
   const int g1 = spmm_grid<T, W>(cpl);
   const int g3 = occ_grid(mk_resid<T, VEC>, kBlock);
   const int g4 = occ_grid(mk_dir<T, VEC>, kBlock);
@@ -797,7 +822,8 @@ int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkRes
     return set_cuda_error("begin capture", e);
   }
   for (int k = 0; k < kHist; ++k) {
-    node(cs, KC_SPMM, b_spmm, [&](cudaStream_t x) { spmm_go<T, W>(cpl, g1, P, x); });
+    if (P.nbh > 0) node(cs, KC_HEAVY, 0.0, [&](cudaStream_t x) { spmm_go<T, W>(1, cpl, g1, P, x); });
+    node(cs, KC_SPMM, b_spmm, [&](cudaStream_t x) { spmm_go<T, W>(2, cpl, g1, P, x); });
     node(cs, KC_RESID, b_resid, [&](cudaStream_t x) { launch_k(mk_resid<T, VEC>, g3, kBlock, 0, x, P, k); });
     node(cs, KC_DIR, b_dir, [&](cudaStream_t x) { launch_k(mk_dir<T, VEC>, g4, kBlock, 0, x, P, k); });
   }

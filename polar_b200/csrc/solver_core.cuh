@@ -76,8 +76,20 @@ POLAR_D void reduce_partials(const double* part, int nblk, int ld, double* tmp, 
   const int S = blockDim.x / ld;
   const int t = threadIdx.x, c = t % ld, s = t / ld;
   if (s < S) {
+    // strip s sums blocks s, s + S, ... in that order; eight loads are issued before the
+    // adds so the strip costs about one L2 round trip per eight partials
+    constexpr int B = 8;
     double acc = 0.0;
-    for (int b = s; b < nblk; b += S) acc += __ldcg(part + (size_t)b * ld + c);
+    for (int b0 = s; b0 < nblk; b0 += B * S) {
+      double v[B];
+#pragma unroll
+      for (int u = 0; u < B; ++u) {
+        const int b = b0 + u * S;
+        v[u] = b < nblk ? __ldcg(part + (size_t)b * ld + c) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < B; ++u) acc += v[u];
+    }
     tmp[s * ld + c] = acc;
   }
   __syncthreads();
