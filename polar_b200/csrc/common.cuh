@@ -69,6 +69,19 @@ POLAR_D void vstore(T* p, const T (&in)[V]) {
   }
 }
 
+// Evict-first (streaming) store, for data that is not read again soon.
+template <typename T, int V>
+POLAR_D void vstore_cs(T* p, const T (&in)[V]) {
+  constexpr int VW = VecWidth<T, V>::value;
+#pragma unroll
+  for (int c = 0; c < V / VW; ++c) {
+    VecU<T, VW> u;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) u.a[i] = in[c * VW + i];
+    __stcs(reinterpret_cast<typename VecType<T, VW>::type*>(p + c * VW), u.v);
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Programmatic dependent launch (sm_90+).  A kernel launched with programmatic stream
 // serialization may start while its predecessor is still running; pdl_wait blocks until

@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
           racc[v] += (double)rv[u][v] * (double)rv[u][v];
         }
         vstore<T, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
-        if (ai[u] >= 0) vstore<T, VEC>(hslot + (size_t)ai[u] * ld + rg.col, rv[u]);
+        if (ai[u] >= 0) vstore_cs<T, VEC>(hslot + (size_t)ai[u] * ld + rg.col, rv[u]);
       }
     }
   }
@@ -503,7 +503,16 @@ __global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ Solv
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
   const double shift0 = __ldg(P.tau);
-  for (long long q = tid; q < (long long)P.p * ld; q += nth) pole_step(P, q, slot, shift0);
+  if (P.cmp) {
+    // pole items spread over the CTAs, one half-warp per item (lane = history index)
+    const int hw = threadIdx.x >> 4, hl = threadIdx.x & 15;
+    const unsigned hmask = 0xffffu << (threadIdx.x & 16);
+    const long long items = (long long)P.p * ld;
+    for (long long q = blockIdx.x + (long long)gridDim.x * hw; q < items; q += (long long)gridDim.x * (blockDim.x >> 4))
+      pole_step_unit(P, q, hl, hmask, slot, shift0);
+  } else {
+    for (long long q = tid; q < (long long)P.p * ld; q += nth) pole_step(P, q, slot, shift0);
+  }
   const bool more = ld_volatile_i32(P.ctl + C_ANY) != 0 && P.stats[0] < P.maxit;
   if (more) {
     const RowGroup rg = make_row_group<VEC>(ld);

@@ -353,6 +353,8 @@ template <> struct FlushAcc<float> { using type = double; };
 
 template <typename T, int E>
 POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool first, bool final_pass, T* sm) {
+  // X, P and the history stream through once per pass: evict-first loads and stores keep
+  // the CG vectors and the graph in L2 across the pass
   using C = typename FlushAcc<T>::type;
   const int ld = P.ld, nA = P.nA, p = P.p;
   const int cw = flush_cw<T>(ld);
@@ -383,7 +385,7 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
     for (int e = 0; e < E; ++e)
 #pragma unroll
       for (int k = 0; k < kHist; ++k)
-        hv[e][k] = arow[e] < nA ? P.hist[((size_t)k * nA + arow[e]) * ld + c] : T(0);
+        hv[e][k] = arow[e] < nA ? __ldcs(P.hist + ((size_t)k * nA + arow[e]) * ld + c) : T(0);
     T w0[E];
 #pragma unroll
     for (int e = 0; e < E; ++e)
@@ -397,8 +399,8 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
       for (int e = 0; e < E; ++e) {
         const bool ok = need && arow[e] < nA;
         const size_t o = ((size_t)j * nA + arow[e]) * ld + c;
-        x[e] = first ? T(0) : (ok ? P.Xb[o] : T(0));
-        pv[e] = first ? w0[e] : ((ok && on) ? P.Pb[o] : T(0));
+        x[e] = first ? T(0) : (ok ? __ldcs(P.Xb + o) : T(0));
+        pv[e] = first ? w0[e] : ((ok && on) ? __ldcs(P.Pb + o) : T(0));
       }
     };
     auto apply = [&](int j, T (&x)[E], T (&pv)[E], bool on) {
@@ -430,7 +432,7 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
         if (!final_pass)
 #pragma unroll
           for (int e = 0; e < E; ++e)
-            if (arow[e] < nA) P.Pb[((size_t)j * nA + arow[e]) * ld + c] = pv[e];
+            if (arow[e] < nA) __stcs(P.Pb + ((size_t)j * nA + arow[e]) * ld + c, pv[e]);
       }
       if (final_pass) {
         if (c < P.R)
@@ -444,7 +446,7 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
       } else {
 #pragma unroll
         for (int e = 0; e < E; ++e)
-          if (arow[e] < nA) P.Xb[((size_t)j * nA + arow[e]) * ld + c] = x[e];
+          if (arow[e] < nA) __stcs(P.Xb + ((size_t)j * nA + arow[e]) * ld + c, x[e]);
       }
     };
     T xa[E], pa[E], xb[E], pb[E];
@@ -521,6 +523,73 @@ POLAR_D void pole_step(const SolvePrm<T>& P, long long q, int slot, double shift
     }
   }
   P.pflag[q] = pf;
+}
+
+// pole_step split over the kHist (= 16) lanes of a half-warp: lane i of the half-warp that
+// holds item q forms the item's step scalars (the same arithmetic as pole_step) and
+// updates only its own composed pair (gamma_i, delta_i); lane 0 also advances the item's
+// recurrence state, this slot's bookkeeping and the coefficient planes, after every lane
+// has read the state (half-warp sync on `hmask`).  Requires P.cmp and kHist == 16.
+template <typename T>
+POLAR_D void pole_step_unit(const SolvePrm<T>& P, long long q, int i, unsigned hmask, int slot, double shift0) {
+  static_assert(kHist == 16, "one half-warp per pole item");
+  const int ld = P.ld;
+  const int j = (int)(q / ld), c = (int)(q % ld);
+  const bool m = P.live[q] && P.upd[c];
+  double* cq = P.cmp + (size_t)q * kNC;
+  const size_t ci = ((size_t)slot * P.p + j) * ld + c;
+  if (!m) {
+    if (slot == 0) {
+      cq[2 + i] = 0.0;
+      cq[2 + kHist + i] = 0.0;
+      if (i == 0) {
+        cq[0] = 0.0;
+        cq[1] = 1.0;
+      }
+    }
+    if (i == 0) {
+      P.ca[ci] = T(0);
+      P.cz[ci] = T(0);
+      P.cb[ci] = T(1);
+      if (slot == 0) P.pflag[q] = 0;
+    }
+    return;
+  }
+  const double theta = __ldg(P.tau + j) - shift0;
+  const double a = P.ag[c], be = P.beg[c], chi = P.chig[c];
+  const double z = P.z[q], zp = P.zp[q];
+  const double zn = z / (1.0 + a * theta + chi * (1.0 - z / zp));
+  const double fac = zn / z;
+  const double aj = a * fac;
+  const double bj = be * fac * fac;
+  if (i < slot) {
+    const double di = cq[2 + kHist + i];
+    cq[2 + i] += aj * di;
+    cq[2 + kHist + i] = bj * di;
+  } else if (slot == 0) {
+    cq[2 + i] = 0.0;
+    if (i > 0) cq[2 + kHist + i] = 0.0;
+  }
+  __syncwarp(hmask);
+  if (i != 0) return;
+  const double beta = slot == 0 ? 1.0 : cq[1];
+  cq[0] = (slot == 0 ? 0.0 : cq[0]) + aj * beta;
+  cq[1] = bj * beta;
+  cq[2 + kHist + slot] = zn;
+  const double rrn = P.rr[c];
+  P.ca[ci] = (T)aj;
+  P.cz[ci] = (T)zn;
+  P.cb[ci] = (T)bj;
+  if (P.track) {
+    const double ipv = P.ip[q], pnv = P.pn[q];
+    P.hs[q] += 2.0 * aj * ipv + aj * aj * pnv;
+    P.ip[q] = bj * (ipv + aj * pnv);
+    P.pn[q] = zn * zn * rrn + bj * bj * pnv;
+  }
+  P.zp[q] = z;
+  P.z[q] = zn;
+  if (fabs(zn) * sqrt(rrn) <= P.stop[c]) P.live[q] = 0;
+  P.pflag[q] = 1;
 }
 
 // Column scalars after the r.r reduction (realworld/polar_gpu.py:103-106, 121-125):
