@@ -124,13 +124,31 @@ def profiled_traffic(config):
 
 
 # ---------------------------------------------------------------------------------------
+def replica_seed(base_seed, rank):
+    """Seed of rank `rank`'s replica graph: replicas run independent greedies."""
+    return base_seed + 1000 * rank
+
+
+def job_seconds(local_s, world, device):
+    """Device time of the whole job: the maximum over ranks (all ranks call this in the
+    same order; a no-op at one rank)."""
+    if world <= 1:
+        return local_s
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([local_s], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
 def build_inputs(a, rank=0):
     from polar_b200.synth import CONFIGS, candidates, chung_lu
     c = dict(CONFIGS[a.config])
     n = a.n or c["n"]
     N = a.N or c["N"]
     k = a.k or c["k"]
-    seed = c["seed"] + 1000 * rank
+    seed = replica_seed(c["seed"], rank)
     E = chung_lu(n, c["mean_deg"], c["gamma"], seed, dmax=c["dmax"] if n == c["n"] else None,
                  min_degree=c.get("min_degree", 0))
     cand = candidates(n, E, N, seed + 7919)
@@ -219,7 +237,7 @@ def run_ours(a):
         ev1.record()
         torch.cuda.synchronize()
     launches = lib.polar_launch_count() - launches0
-    total_s = ev0.elapsed_time(ev1) / 1e3
+    total_s = job_seconds(ev0.elapsed_time(ev1) / 1e3, world, dev)
     # ---- one more greedy with every solver kernel bracketed by CUDA events (the event
     # nodes serialise the iteration graph, so this run is not part of `value`) ----
     torch.cuda.synchronize()
@@ -227,11 +245,6 @@ def run_ours(a):
     inst = timed_run("mixed")
     ktime = _lib.kernel_timing()
     lib.polar_set_kernel_timing(0)
-    if world > 1:
-        t = torch.tensor([total_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_s = float(t.item())
-        dist.barrier()
     per = total_s / a.steps
     mixed = runs[-1]
 

@@ -49,10 +49,10 @@ POLAR_D RowGroup make_row_group(int ld) {
 // cooperatively and broadcast them by shuffles; narrower groups read the next 4 indices
 // directly (the same addresses for the group's lanes, served by L1) so 4 gathers are in
 // flight per lane.
-template <typename T, int VEC, bool WEIGHTED>
+template <typename T, int VEC, bool WEIGHTED, typename AA = typename AccOf<T>::type>
 POLAR_D void gather_rows(const polar_graph& g, const RowGroup& rg, int lo, int hi, const T* X,
-                         int ld, typename AccOf<T>::type (&acc)[VEC], bool on = true) {
-  using A = typename AccOf<T>::type;
+                         int ld, AA (&acc)[VEC], bool on = true) {
+  using A = AA;
   if (rg.G < 4) {
     if (!on) return;
     int k = lo;
@@ -152,17 +152,18 @@ POLAR_D double added_terms(const polar_graph& g, const RowGroup& rg, int i, cons
 
 // Finishes row i from its own entries xi (already loaded): y = (diag + shift) x_i - acc.
 // ADD = false leaves out the added edges (the caller applies them afterwards).
-template <typename T, int VEC, bool ADD = true>
+template <typename T, int VEC, bool ADD = true, typename AA = typename AccOf<T>::type>
 POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int deg, double shift, const T* X,
-                            int ld, typename AccOf<T>::type (&acc)[VEC], T* Y, int ldy, const T (&xi)[VEC],
+                            int ld, AA (&acc)[VEC], T* Y, int ldy, const T (&xi)[VEC],
                             T (&yi)[VEC], bool store = true) {
-  using A = typename AccOf<T>::type;
+  using A = AA;
   if (!store) {
 #pragma unroll
     for (int v = 0; v < VEC; ++v) yi[v] = T(0);
     return;
   }
-  const double wadd = ADD ? added_terms<T, VEC>(g, rg, i, X, ld, acc) : 0.0;
+  double wadd = 0.0;
+  if constexpr (ADD) wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
 #pragma unroll
   for (int v = 0; v < VEC; ++v) yi[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
@@ -170,17 +171,18 @@ POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int
 }
 
 // Finishes row i: y = (diag + shift) x_i - acc.  Returns x_i in xi (for d^T v).
-template <typename T, int VEC, bool ADD = true>
+template <typename T, int VEC, bool ADD = true, typename AA = typename AccOf<T>::type>
 POLAR_D void finish_row(const polar_graph& g, const RowGroup& rg, int i, int deg, double shift,
-                        const T* X, int ld, typename AccOf<T>::type (&acc)[VEC], T* Y,
+                        const T* X, int ld, AA (&acc)[VEC], T* Y,
                         int ldy, T (&xi)[VEC], T (&yi)[VEC], bool store = true) {
-  using A = typename AccOf<T>::type;
+  using A = AA;
   if (!store) {  // lane idle: nothing to compute
 #pragma unroll
     for (int v = 0; v < VEC; ++v) xi[v] = yi[v] = T(0);
     return;
   }
-  const double wadd = ADD ? added_terms<T, VEC>(g, rg, i, X, ld, acc) : 0.0;
+  double wadd = 0.0;
+  if constexpr (ADD) wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
   vload<T, VEC>(xi, X + (size_t)i * ld + rg.col);
 #pragma unroll

@@ -384,7 +384,7 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
   add((size_t)kHist * nA * ld * ts);               // 3 hist
   add((size_t)p * nA * ld * ts);                   // 4 P
   add((size_t)p * nA * ld * ts);                   // 5 X
-  add((size_t)(g->nchunks > 0 ? g->nchunks : 1) * ld * ts);  // 6 chunk partials
+  add((size_t)(g->nchunks > 0 ? g->nchunks : 1) * ld * 8);   // 6 chunk partials (FP64 sums)
   add((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 * (ld > 16 ? ld / 16 : 1));  // 7 heavy counters per panel
   add((size_t)grid * ld * 8);                      // 8 CTA partials
   for (int i = 0; i < 6; ++i) add((size_t)ld * 8);  // 9..14 rr stop ap bp a be

@@ -21,6 +21,7 @@
 #include <vector>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 
 #include "common.cuh"
 #include "graph_ops.cuh"
@@ -150,6 +151,16 @@ POLAR_D void apply_added_edges(const SolvePrm<T>& P, double* tmp, double* s_col)
 #ifndef POLAR_RESID_U
 #define POLAR_RESID_U 2   // same for the r update (more spills at 64 registers)
 #endif
+// SpMM accumulator: FP64 row sums for FP32 vectors unless POLAR_SPMM_ACC64 = 0.  A
+// Laplacian row (deg + sigma + shift) x_i - sum_j x_j cancels heavily for smooth vectors, so
+// the neighbour sum is kept unrounded until that final combination (one rounding per row
+// instead of one per neighbour).  This bounds the mixed path's marginal error below 1e-6.
+#ifndef POLAR_SPMM_ACC64
+#define POLAR_SPMM_ACC64 1
+#endif
+template <typename T> struct SpmmAcc { using type = double; };
+template <> struct SpmmAcc<float> { using type = std::conditional<POLAR_SPMM_ACC64 != 0, double, float>::type; };
+
 #ifndef POLAR_HEAVY_BYTES
 #define POLAR_HEAVY_BYTES 64
 #endif
@@ -168,7 +179,8 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
   pdl_wait();
   pdl_launch();
   if (!solve_live(P.ctl, P.stats, P.maxit)) return;
-  using A = typename AccOf<T>::type;
+  using A = typename SpmmAcc<T>::type;
+  A* const chunk_part = reinterpret_cast<A*>(P.chunk_part);
   __shared__ double red[kWarps * kMaxLd];
   __shared__ double s_col[kMaxLd];
   const polar_graph& g = P.g;
@@ -248,7 +260,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       if (single) {
         if (grp == 0) {
           T yi[CPL];
-          finish_row_pre<T, CPL, false>(g, rg, i, cnt, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
+          finish_row_pre<T, CPL, false, A>(g, rg, i, cnt, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
           if (on)
 #pragma unroll
             for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
@@ -256,7 +268,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
         continue;
       }
       if (on && grp == 0) {
-        vstore<A, CPL>(P.chunk_part + (size_t)ch * ld + rg.col, acc);
+        vstore<A, CPL>(chunk_part + (size_t)ch * ld + rg.col, acc);
 #pragma unroll
         for (int v = 0; v < CPL; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
         if (ch == c0) {
@@ -279,13 +291,13 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
         if (on)
           for (int c2 = c0; c2 < c1; ++c2) {
             A pv[CPL];
-            vload_cg<A, CPL>(pv, P.chunk_part + (size_t)c2 * ld + rg.col);
+            vload_cg<A, CPL>(pv, chunk_part + (size_t)c2 * ld + rg.col);
 #pragma unroll
             for (int v = 0; v < CPL; ++v) sum[v] += pv[v];
           }
         const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
         T xf[CPL], yi[CPL];
-        finish_row<T, CPL, false>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
+        finish_row<T, CPL, false, A>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
         if (lane == 0) P.hcount[h] = 0;
       }
       __syncwarp();
@@ -398,8 +410,8 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       A acc[CPL];
 #pragma unroll
       for (int v = 0; v < CPL; ++v) acc[v] = A(0);
-      gather_rows<T, CPL, W>(g, rg, lo, hi, P.d, ld, acc, on);
-      finish_row_pre<T, CPL, false>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
+      gather_rows<T, CPL, W, A>(g, rg, lo, hi, P.d, ld, acc, on);
+      finish_row_pre<T, CPL, false, A>(g, rg, i, hi - lo, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
       if (!on)
 #pragma unroll
         for (int v = 0; v < CPL; ++v) xi[v] = T(0);
