@@ -404,3 +404,46 @@ def true_marginals(G, cand, seq, s, obj="frac", eps=1e-9, tol=1e-10, kmax=None, 
         op.add(a, b)
     rho = tol * float(np.max((G.Lam(kmax) + tau) / (G.sigma + tau)))
     return np.array(out), dict(quadrature_bound=qerr, residual_rho=rho, p=len(tau), spmv=cnt.spmv)
+
+
+# ---------------------------------------------------------------------------------------
+# Relaxed-weight objective (the differentiation path).  No counterpart in the reference:
+# its oracle is the dense FP64 eigendecomposition, plus the same positive Stieltjes rule
+# evaluated densely so that the device path can be checked with the rule's error removed.
+def relaxed_dense(n, edges, sigma, cand, w, s, tau=None, om=None):
+    """Exact f_s(w, sigma) = Tr(A_0^{-s}) - Tr(A_w^{-s}), d f/d w_e = s b_e^T A_w^{-s-1} b_e
+    and d f/d sigma = -s (Tr(A_0^{-s-1}) - Tr(A_w^{-s-1})) from eigendecompositions, with
+    A_0 = L + sigma I, A_w = A_0 + sum_e w_e b_e b_e^T.  With (tau, om), also the rule's
+    values: f_q = sum_j om_j phi(tau_j), g_q = sum_j om_j ||(A_w + tau_j)^{-1} b_e||^2 and
+    ds_q = -s sum_j (om_j / tau_j)(phi(0) - phi(tau_j)), where
+    phi(t) = Tr((A_0 + t)^{-1}) - Tr((A_w + t)^{-1})."""
+    edges = np.asarray(edges, np.int64).reshape(-1, 2)
+    cand = np.asarray(cand, np.int64).reshape(-1, 2)
+    w = np.asarray(w, np.float64)
+    A0 = np.zeros((n, n))
+    for a, b in edges:
+        A0[a, a] += 1.0
+        A0[b, b] += 1.0
+        A0[a, b] -= 1.0
+        A0[b, a] -= 1.0
+    A0 += sigma * np.eye(n)
+    Aw = A0.copy()
+    for (a, b), we in zip(cand, w):
+        Aw[a, a] += we
+        Aw[b, b] += we
+        Aw[a, b] -= we
+        Aw[b, a] -= we
+    l0 = np.linalg.eigvalsh(A0)
+    lw, V = np.linalg.eigh(Aw)
+    D = V[cand[:, 0]] - V[cand[:, 1]]  # (m, n): b_e^T v_i
+    out = dict(f=float(np.sum(l0 ** -s) - np.sum(lw ** -s)),
+               grad=s * (D ** 2) @ (lw ** (-s - 1)),
+               dsigma=float(-s * (np.sum(l0 ** (-s - 1)) - np.sum(lw ** (-s - 1)))))
+    if tau is not None:
+        tau = np.asarray(tau, np.float64)
+        om = np.asarray(om, np.float64)
+        phi = lambda t: np.sum(1.0 / (l0 + t)) - np.sum(1.0 / (lw + t))
+        out["f_q"] = float(sum(o * phi(t) for t, o in zip(tau, om)))
+        out["grad_q"] = np.array([sum(o * np.sum((d / (lw + t)) ** 2) for t, o in zip(tau, om)) for d in D])
+        out["dsigma_q"] = float(-s * sum((o / t) * (phi(0.0) - phi(t)) for t, o in zip(tau, om)))
+    return out

@@ -5,6 +5,8 @@ Drop-in for the entry points of realworld/polar_gpu.py that the drivers call
 true_marginals, degree_greedy, random_set, chunk_width.  The compute runs in the
 hand-written kernels of libpolar.so (include/polar.h) through ctypes; there is no CPU
 fallback.  Keyword-only extensions: precision='fp64'|'mixed', K=<fixed pole count>.
+Beyond the reference: FracTrace / relaxed_gradient / relaxed_objective, the relaxed-weight
+objective f_s(w, sigma) with its adjoint (polar_b200.adjoint).
 """
 from .quadrature import composite, fixed_rule, poles
 from .sketch import sketches, chunk_width
@@ -12,7 +14,8 @@ from .synth import chung_lu, candidates
 
 __version__ = "0.1.0"
 
-_DEVICE_NAMES = ("Graph", "Op", "msolve", "Counter", "polar", "true_marginals", "degree_greedy", "random_set")
+_DEVICE_NAMES = ("Graph", "Op", "msolve", "Counter", "polar", "true_marginals", "degree_greedy", "random_set",
+                 "FracTrace", "relaxed_gradient", "relaxed_objective")
 
 
 def __getattr__(name):
@@ -27,6 +30,9 @@ def __getattr__(name):
     if name in ("polar", "true_marginals", "degree_greedy", "random_set"):
         from . import greedy
         return getattr(greedy, name)
+    if name in ("FracTrace", "relaxed_gradient", "relaxed_objective"):
+        from . import adjoint
+        return getattr(adjoint, name)
     raise AttributeError(name)
 
 
