@@ -48,6 +48,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=1, help="oracle CG iterations timed per width")
     ap.add_argument("--phases", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the solver's default SpMM layouts")
+    ap.add_argument("--quick", action="store_true", help="full-n4M: one short solve (an ncu-sized case)")
+    ap.add_argument("--cache", default=None, help="full-n4M: .npz file holding the generated edge list "
+                                                    "(written when absent, read when present)")
     return ap.parse_args()
 
 
@@ -210,6 +214,16 @@ def run_ours(a):
     G = pg.Graph(n, E, c["sigma"])
     sk = pg.sketches(G, cand, c["q"], 2026)
     kw = dict(q=c["q"], B=c["B"], tol=c["tol"], sketch=sk, K=c["K"])
+    tuned = {}
+    if not a.no_autotune:
+        # SpMM layout per solve width (shortlist B, bank 2q), timed once before any greedy
+        from polar_b200 import autotune
+        for prec, wide in (("mixed", 128), ("fp64", 64)):
+            for R in sorted({c["B"], min(2 * c["q"], wide)}):
+                t = autotune.tune_msolve(pg.Op(G), R, prec, p=c["K"])
+                tuned[f"{prec}_R{R}"] = {"lane_bytes": t["best"][0], "sliced_ell": t["best"][1],
+                                         "heavy_thresh": t["best"][2], "us_per_iter": t["us_per_iter"],
+                                         "layouts_timed": len(t["table"])}
 
     def timed_run(prec, **extra):
         torch.cuda.synchronize()
@@ -300,7 +314,8 @@ def run_ours(a):
         line = {
             "metric": METRIC, "value": per, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": per * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 vectors, f64 scalars", "data": "synthetic (seeded Chung-Lu stand-in for com-DBLP shape)",
+            "dtype": "f32 SpMM input/output and pole iterates; f64 residual, direction and scalars",
+            "data": "synthetic (seeded Chung-Lu stand-in for com-DBLP shape)",
             "config": {"workload": a.config, "n": n, "m": int(len(E)), "N": N, "K": c["K"], "q": c["q"],
                        "B": c["B"], "k": k, "s": c["s"], "sigma": c["sigma"], "tol": c["tol"],
                        "l2": "inputs larger than L2 (X/Y banks 2.8 GB, SpMM block 162 MB)",
@@ -320,12 +335,221 @@ def run_ours(a):
             "spmv": mixed["spmv"], "p": mixed["p"],
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "autotune": tuned or None,
         }
         if a.phases:
             line["phases"] = mixed.get("phases")
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_batch(a):
+    """Many-graphs workload: the bank solves of 48 graphs (2q right-hand sides each, K poles
+    from each graph's own s and sigma) in one polar_msolve_batch launch, against the same
+    solves one graph at a time through msolve."""
+    import torch
+
+    import polar_b200 as pg
+    from polar_b200 import _lib
+    from polar_b200.batch import msolve_batch
+    from polar_b200.synth import CONFIGS, batch_specs, candidates, chung_lu
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    c = CONFIGS["batch48"]
+    specs = batch_specs(c["graphs"])
+    R = 2 * c["q"]
+    t_gen = time.perf_counter()
+    ops, Ws, taus, acts, Wh, meta = [], [], [], [], [], []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(2026)
+    for sp in specs:
+        n = min(sp["n"], a.n) if a.n else sp["n"]
+        E = chung_lu(n, sp["mean_deg"], sp["gamma"], sp["seed"], min_degree=1)
+        cand = candidates(n, E, min(c["N"], n), sp["seed"] + 7919)
+        G = pg.Graph(n, E, sp["sigma"])
+        tau, _, _ = pg.poles("frac", sp["s"], sp["sigma"], G.Lam(c["k"]), 1e-2, K=c["K"])
+        W = torch.randn((n, R), generator=gen, device=dev, dtype=torch.float64) / np.sqrt(c["q"])
+        ops.append(pg.Op(G))
+        Ws.append(W)
+        taus.append(tau)
+        acts.append(np.unique(cand))
+        meta.append((n, G.nnz))
+    t_gen = time.perf_counter() - t_gen
+    kw = dict(precision="mixed")
+
+    def batch_once(W_list):
+        return msolve_batch(ops, W_list, taus, acts, c["tol"], **kw)
+
+    for _ in range(a.warmup):
+        res = batch_once(Ws)
+    torch.cuda.synchronize()
+    launches0 = lib.polar_launch_count()
+    with Clocks(0) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            res = batch_once(Ws)
+        e1.record()
+        torch.cuda.synchronize()
+    launches = lib.polar_launch_count() - launches0
+    per = e0.elapsed_time(e1) / 1e3 / a.steps
+    iters = [int(it.max()) for _, _, it in res]
+    colit = sum(int(it.sum()) for _, _, it in res)
+    # the same solves one graph at a time (kernel-per-phase driver, CUDA-graph blocks)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    seq = [pg.msolve(ops[g], Ws[g], taus[g], acts[g], c["tol"], **kw) for g in range(len(ops))]
+    s1.record()
+    torch.cuda.synchronize()
+    seq_s = s0.elapsed_time(s1) / 1e3
+    err = max(float((X.double() - Xs.double()).abs().max() / Xs.double().abs().max().clamp_min(1e-300))
+              for (X, _, _), (Xs, _, _) in zip(res, seq))
+    # end to end: host right-hand sides in, host solutions out
+    Wh = [W.cpu().numpy() for W in Ws]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = batch_once(Wh)
+    Xh = [X.cpu() for X, _, _ in out]
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(W.nbytes for W in Wh)
+    d2h = sum(X.numel() * X.element_size() for X in Xh)
+    # bytes moved by the SpMM and vector phases, per seed iteration (algorithmic, FP32)
+    alg = sum(it * (4.0 * (n + 1) + 4.0 * nnz + 2 * 4.0 * n * R + 6 * 4.0 * n * R)
+              for it, (n, nnz) in zip(iters, meta))
+    line = {
+        "metric": "batched bank solves of 48 graphs (mixed precision)", "value": per, "unit": "s/batch",
+        "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "ms_per_step": per * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 SpMM input/output and pole iterates; f64 residual, direction and scalars",
+        "data": "synthetic (48 seeded Chung-Lu graphs, Gaussian right-hand sides)",
+        "config": {"workload": "batch48", "graphs": len(ops), "n_total": int(sum(m[0] for m in meta)),
+                   "nnz_total": int(sum(m[1] for m in meta)), "K": c["K"], "R": R, "N_per_graph": c["N"],
+                   "tol": c["tol"], "l2": "inputs larger than L2 (block vectors of all graphs: %.1f GB)"
+                   % (sum(m[0] for m in meta) * R * 4 * 3 / 1e9)},
+        "sequential_s": seq_s, "batch_speedup_vs_sequential": seq_s / per,
+        "max_rel_diff_vs_sequential": err, "seed_iterations": {"max": max(iters), "sum": sum(iters)},
+        "column_iterations_per_s": colit / per, "alg_GBps": alg / per / 1e9,
+        "e2e": {"value": e2e_s, "unit": "s/batch", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches), "clocks": clk.summary(), "host_setup_s": t_gen,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_full(a):
+    """Full-scale solve: the shortlist solve of the n = 4.0M / 34.7M-edge workload (B = 16
+    incidence columns, K = 32 poles, tol 1e-6, pole iterates on ~1.57M active rows) in FP64
+    and in mixed precision, with the per-kernel table of each; plus the SpMM alone at 16 and
+    64 columns.  `--quick` runs only a 48-iteration mixed solve over 32 active rows (the
+    small case for an ncu capture of the SpMM)."""
+    import torch
+
+    import polar_b200 as pg
+    from polar_b200 import _lib
+    from polar_b200.synth import CONFIGS, candidates, chung_lu
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    lib = _lib.load()
+    c = CONFIGS["full-n4M"]
+    n = a.n or c["n"]
+    t_gen = time.perf_counter()
+    if a.cache and os.path.exists(a.cache):
+        E = np.load(a.cache)["edges"].astype(np.int64)
+    else:
+        E = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=c["dmax"] if n == c["n"] else None,
+                     min_degree=c["min_degree"])
+        if a.cache:
+            np.savez(a.cache, edges=E.astype(np.int32))
+    pairs = candidates(n, E, c["B"], c["seed"] + 7919)
+    rng = np.random.default_rng(c["seed"])
+    # endpoints of N uniform candidate pairs: the active rows of the workload's pole iterates
+    Nq = 16 if a.quick else c["N"]
+    active = np.unique(np.concatenate([rng.integers(0, n, 2 * Nq), pairs.ravel()]))
+    G = pg.Graph(n, E, c["sigma"])
+    t_gen = time.perf_counter() - t_gen
+    op = pg.Op(G)
+    tau, om, _ = pg.poles("frac", c["s"], c["sigma"], G.Lam(c["k"]), 1e-2, K=c["K"])
+    R = c["B"]
+    W = np.zeros((n, R))
+    W[pairs[:, 0], np.arange(R)] = 1.0
+    W[pairs[:, 1], np.arange(R)] = -1.0
+    Wd = torch.as_tensor(W).to(dev)
+    from polar_b200 import solver as S
+    act_d, pos_d = S.prepare_active(active, n, dev)
+    ia = np.searchsorted(active, pairs[:, 0])
+    ib = np.searchsorted(active, pairs[:, 1])
+
+    def solve(prec, maxit=100000):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        try:
+            X, h, it = S.msolve(op, Wd, tau, act_d, c["tol"], maxit=maxit, track=True, precision=prec,
+                                active_pos=pos_d)
+        except _lib.PolarError as e:
+            if e.status != _lib.POLAR_ERR_ITER_CAP or maxit == 100000:
+                raise
+            return None
+        e1.record()
+        torch.cuda.synchronize()
+        cols = torch.arange(R, device=dev)
+        bu = (X[:, torch.as_tensor(ia, device=dev), cols].double()
+              - X[:, torch.as_tensor(ib, device=dev), cols].double()).cpu().numpy()
+        G_q = (om[:, None] * h.cpu().numpy() / (1.0 + bu)).sum(0)
+        return {"seconds": e0.elapsed_time(e1) / 1e3, "iterations": int(it.max()), "G": G_q}
+
+    if a.quick:
+        lib.polar_set_kernel_timing(1)
+        solve("mixed", maxit=48)
+        kt = _lib.kernel_timing()
+        lib.polar_set_kernel_timing(0)
+        print(json.dumps({"workload": "full-n4M", "quick": True, "n": n, "nnz": G.nnz,
+                          "spmm_ms_per_launch": kt["spmm"][1] / max(1, kt["spmm"][0])}), flush=True)
+        return
+    out = {}
+    for prec in ("fp64", "mixed"):
+        solve(prec, maxit=16)  # warm-up: graph partitions, workspace, CUDA graphs
+        res = solve(prec)
+        lib.polar_set_kernel_timing(1)
+        inst = solve(prec)
+        kt = _lib.kernel_timing()
+        lib.polar_set_kernel_timing(0)
+        out[prec] = dict(res, kernels={k: {"launches": v[0], "ms": v[1],
+                                           "alg_GBps": v[2] / (v[1] / 1e3) / 1e9 if v[1] > 0 else None}
+                                       for k, v in kt.items() if v[0]},
+                         instrumented_seconds=inst["seconds"])
+    G64, G32 = out["fp64"].pop("G"), out["mixed"].pop("G")
+    # the SpMM alone (polar_spmm through Op), 16 and 64 columns, both precisions
+    hbm, peak_kind = peak_hbm()
+    spmm = {}
+    for dt, nm in ((torch.float64, "fp64"), (torch.float32, "mixed")):
+        for Rc in (16, 64):
+            Xs = torch.randn((n, Rc), device=dev, dtype=torch.float64).to(dt)
+            op(Xs, 0.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 10
+            e0.record()
+            for _ in range(reps):
+                op(Xs, 0.0)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            el = 8 if dt == torch.float64 else 4
+            alg = 4.0 * (n + 1) + 4.0 * G.nnz + 2.0 * el * n * Rc
+            spmm[f"{nm}_R{Rc}"] = {"ms": ms, "alg_GBps": alg / (ms / 1e3) / 1e9,
+                                   "frac_of_peak": alg / (ms / 1e3) / 1e9 / hbm}
+            del Xs
+    line = {"metric": "full-scale shortlist solve (B = 16 columns, K = 32 poles)", "unit": "s/solve",
+            "value": out["mixed"]["seconds"], "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": "full-n4M", "n": n, "m": int(len(E)), "nnz": G.nnz, "dmax": G.dmax,
+                       "nA": int(len(active)), "K": c["K"], "R": R, "tol": c["tol"], "sigma": c["sigma"], "s": c["s"]},
+            "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_speedup_vs_fp64": out["fp64"]["seconds"] / out["mixed"]["seconds"],
+            "max_rel_marginal_err": float(np.max(np.abs(G32 - G64) / np.abs(G64))),
+            "spmm_alone": spmm, "peak_GBps": hbm, "peak_source": peak_kind, "host_setup_s": t_gen}
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(a):
@@ -396,7 +620,16 @@ def run_reference(a):
 
 if __name__ == "__main__":
     args = parse()
-    if args.impl == "reference":
+    if args.impl == "reference" and args.config in ("batch48", "full-n4M"):
+        why = {"batch48": "the many-graphs workload has no reference arm: the reference solves one graph per call",
+               "full-n4M": "the full-scale solve has no reference arm here: the oracle's FP64 NumPy solve of a "
+                           "4M-vertex graph takes hours on the host cores"}[args.config]
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+    elif args.impl == "reference":
         run_reference(args)
+    elif args.config == "batch48":
+        run_batch(args)
+    elif args.config == "full-n4M":
+        run_full(args)
     else:
         run_ours(args)

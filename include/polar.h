@@ -119,8 +119,9 @@ int polar_version(void);
  * class 0 SpMM (light rows), 6 SpMM heavy-row launch, 1 residual update,
  * 2 direction/pole update, 3 deferred update, 4 init, the number of timed launches, their
  * summed device time (ms) and summed algorithmic bytes (SpMM, both launches together,
- * counted on class 0: 4(n+1) + 4 nnz + 2 s n R; residual: 3 s n R + s nA R; direction:
- * 3 s n R; deferred update: (4p + M) s nA R). */
+ * counted on class 0: 4(n+1) + 4 nnz + 2 s n R; residual, r in FP64: (16 + s) n R + s nA R;
+ * direction: 24 n R in FP64, 28 n R in mixed precision (FP64 r and direction in, FP64
+ * direction and its FP32 copy out); deferred update: (4p + M) s nA R). */
 long long polar_launch_count(void);
 void polar_set_kernel_timing(int on);
 int polar_kernel_timing(int cls, long long* launches, double* ms, double* bytes);
@@ -178,6 +179,41 @@ int polar_sell_rows(int precision, int R);
 void polar_set_spmm_lane_bytes(int bytes);
 /* 1 (default): polar_sell_rows reports the sliced-ELL height the solver uses; 0: CSR rows. */
 void polar_set_sell(int on);
+
+/* ---- batched multi-shift solves (many graphs at once) ----
+ * Replaces a loop of realworld/polar_gpu.py:88-133 (msolve) calls, one per graph: the
+ * reference solves one graph per call.  Each problem carries exactly the arguments of
+ * polar_msolve (its own graph, right-hand sides, poles, active rows, tolerance and
+ * outputs) and its own workspace of polar_msolve_batch_workspace_bytes.  All problems of a
+ * batch share the precision, the padded width (next power of two of R) and weighted-ness;
+ * each graph's partition uses polar_heavy_threshold / polar_sell_rows as for polar_msolve.
+ * Driver 0 (default): every problem's solve runs on its own stream (ordered after
+ * `stream`), with its grids scaled to its rows, and the host relaunches each solve's
+ * iteration block as soon as the previous one drains; the call returns when all are done.
+ * Driver 1 (polar_set_solver_mode(1)): one cooperative launch of the persistent solver;
+ * problem b gets a share of the co-resident CTAs in proportion to `cost` (<= 0:
+ * (nnz + 2n) * width / sqrt(sigma)), and its CTAs synchronise only among themselves, with
+ * the same bounded waits as polar_msolve; at most as many problems as co-resident CTAs.
+ * At most 64 problems.  polar_msolve_finish(d_workspace of problem b) returns problem b's
+ * status and statistics. */
+typedef struct polar_msolve_problem {
+  const polar_graph* g;     /* host pointer, read during the call */
+  const double* d_W;        /* n x R FP64, ldw */
+  const double* d_tau;      /* p */
+  const int32_t* d_active;  /* nA, ascending */
+  const int32_t* d_active_pos; /* n: row -> active index or -1 */
+  void* d_X_out;            /* [p][nA][ldx], float when x_f32 else double */
+  double* d_h_out;          /* [p][R] when track, else NULL */
+  int64_t* d_iters_out;     /* R */
+  void* d_workspace;
+  size_t workspace_bytes;
+  double tol;
+  int64_t maxit;
+  double cost;              /* relative work for the CTA split; <= 0: estimated */
+  int32_t ldw, R, p, nA, track, x_f32, ldx, pad;
+} polar_msolve_problem;
+size_t polar_msolve_batch_workspace_bytes(const polar_graph* g, int precision, int R, int p, int nA);
+int polar_msolve_batch(const polar_msolve_problem* probs, int nprob, int precision, polar_stream_t stream);
 
 /* ---- incidence right-hand sides (polar_gpu.py:225-226, 282) ----
  * For c < R with e = sel[c] and (a, b) = cand[e] (cand: int64 [N][2]):

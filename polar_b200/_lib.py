@@ -65,6 +65,18 @@ _S = ctypes.c_size_t
 _I64 = ctypes.c_int64
 _GP = ctypes.POINTER(PolarGraph)
 
+
+class MsolveProblem(ctypes.Structure):
+    """polar_msolve_problem: one solve of a polar_msolve_batch call (polar_msolve's arguments)."""
+    _fields_ = [
+        ("g", _GP), ("d_W", _P), ("d_tau", _P), ("d_active", _P), ("d_active_pos", _P), ("d_X_out", _P),
+        ("d_h_out", _P), ("d_iters_out", _P), ("d_workspace", _P), ("workspace_bytes", _S),
+        ("tol", _D), ("maxit", _I64), ("cost", _D),
+        ("ldw", ctypes.c_int32), ("R", ctypes.c_int32), ("p", ctypes.c_int32), ("nA", ctypes.c_int32),
+        ("track", ctypes.c_int32), ("x_f32", ctypes.c_int32), ("ldx", ctypes.c_int32), ("pad", ctypes.c_int32),
+    ]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "polar_last_error": (ctypes.c_char_p, []),
@@ -86,6 +98,8 @@ SIGNATURES = {
     "polar_sell_rows": (_I, [_I, _I]),
     "polar_set_spmm_lane_bytes": (None, [_I]),
     "polar_set_sell": (None, [_I]),
+    "polar_msolve_batch_workspace_bytes": (_S, [_GP, _I, _I, _I, _I]),
+    "polar_msolve_batch": (_I, [ctypes.POINTER(MsolveProblem), _I, _I, _P]),
     "polar_fill_incidence": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
     "polar_pair_norms": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _P]),
     "polar_topb_tmp_bytes": (_S, [_I, _I]),

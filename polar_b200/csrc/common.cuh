@@ -114,13 +114,16 @@ POLAR_D int ld_volatile_i32(const int* p) { return *reinterpret_cast<const volat
 // writes and bumps `count`; the last CTA to arrive may run serial work (a reduction of
 // per-CTA partials) before it releases the others by advancing `gen`.  Waiting CTAs
 // poll `gen` with a time limit; on expiry they record POLAR_ERR_TIMEOUT in `err` and
-// every CTA leaves the kernel at its next barrier.  No wait is unbounded.
+// every CTA leaves the kernel at its next barrier.  No wait is unbounded.  `nblk` is the
+// number of CTAs that take part: the whole grid, or one problem's share of the CTAs of a
+// batched launch (each share has its own count/gen words).
 struct GridSync {
   unsigned* count;
   unsigned* gen;
   int* err;
   int* where;
   uint64_t timeout_ns;
+  unsigned nblk;
 };
 
 // Returns true in every thread of the last-arriving CTA.  `my_gen` receives the
@@ -133,7 +136,7 @@ POLAR_D bool grid_arrive(const GridSync& s, unsigned& my_gen) {
     unsigned g = ld_acquire_u32(s.gen);
     __threadfence();
     unsigned old = atomicAdd(s.count, 1u);
-    sh_last = (old == gridDim.x - 1) ? 1u : 0u;
+    sh_last = (old == s.nblk - 1) ? 1u : 0u;
     sh_gen = g;
     if (sh_last) __threadfence();
   }

@@ -294,7 +294,10 @@ POLAR_D void stream_block(const polar_graph& g, const RowGroup& rg, int r0, int 
 // memory (red[warp][c]) in a fixed order.
 template <typename T, int VEC, bool WEIGHTED, bool DOT>
 POLAR_D void spmm_phase(const polar_graph& g, int ld, double shift, const T* X, T* Y, int ldy,
-                        typename AccOf<T>::type* chunk_part, int* hcount, double* red, const int* act) {
+                        typename AccOf<T>::type* chunk_part, int* hcount, double* red, const int* act,
+                        int vb = -1, int vnb = -1) {
+  // (vb, vnb): this CTA's index among the CTAs sharing the work, and their count
+  // (default: blockIdx.x of gridDim.x)
   using A = typename AccOf<T>::type;
   constexpr int PANEL = POLAR_PANEL_BYTES / sizeof(T);
   const int pw = ld < PANEL ? ld : PANEL;
@@ -308,8 +311,8 @@ POLAR_D void spmm_phase(const polar_graph& g, int ld, double shift, const T* X, 
   const int gpw = 32 / rg.G;
   const int grp = lane / rg.G;
   const int wpb = blockDim.x >> 5;
-  const int gwarp = blockIdx.x * wpb + warp;
-  const int nwarps = gridDim.x * wpb;
+  const int gwarp = (vb < 0 ? (int)blockIdx.x : vb) * wpb + warp;
+  const int nwarps = (vnb < 0 ? (int)gridDim.x : vnb) * wpb;
   const int gid = gwarp * gpw + grp;
   const int GT = nwarps * gpw;
   if (DOT) {

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "graph_ops.cuh"
@@ -34,8 +35,11 @@
 namespace polar {
 
 // ---------------------------------------------------------------------------------------
+// The whole solve for one problem on `vnb` co-resident CTAs; this CTA is number `vb` of
+// them.  The CTAs of a problem synchronise only among themselves (barrier words in the
+// problem's own control block).
 template <typename T, int VEC, bool WEIGHTED, int E>
-__global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
+POLAR_D void msolve_run(const SolvePrm<T>& P, const int vb, const int vnb) {
   __shared__ double red[kWarps * kMaxLd];
   __shared__ double s_col[2][kMaxLd];
 
@@ -45,17 +49,16 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
   gs.err = P.ctl + 1;
   gs.where = P.ctl + 2;
   gs.timeout_ns = P.timeout_ns;
+  gs.nblk = (unsigned)vnb;
 
   const int ld = P.ld, p = P.p, n = P.n, nA = P.nA;
   const RowGroup rg = make_row_group<VEC>(ld);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gpw = 32 / rg.G;
-  const int gid = (blockIdx.x * kWarps + warp) * gpw + lane / rg.G;
-  const int GT = gridDim.x * kWarps * gpw;
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nth = (long long)gridDim.x * blockDim.x;
+  const long long tid = (long long)vb * blockDim.x + threadIdx.x;
+  const long long nth = (long long)vnb * blockDim.x;
   const long long nvec = (long long)n * rg.G;  // VEC-vectors in an n x ld block
-  double* my_part = P.part + (size_t)blockIdx.x * ld;
+  double* my_part = P.part + (size_t)vb * ld;
 
   // ---- P0: r = d = W, partial r.r ----
   {
@@ -64,14 +67,17 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
     for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
     for (long long e = tid; e < nvec; e += nth) {
       const long long i = e / rg.G;
+      double wd[VEC];
       T w[VEC];
 #pragma unroll
       for (int v = 0; v < VEC; ++v) {
         const int c = rg.col + v;
-        w[v] = (c < P.R) ? (T)__ldg(P.W + (size_t)i * P.ldw + c) : T(0);
-        acc[v] += (double)w[v] * (double)w[v];
+        wd[v] = (c < P.R) ? __ldg(P.W + (size_t)i * P.ldw + c) : 0.0;
+        w[v] = (T)wd[v];
+        acc[v] += wd[v] * wd[v];
       }
-      vstore<T, VEC>(P.r + (size_t)i * ld + rg.col, w);
+      vstore<double, VEC>(P.r + (size_t)i * ld + rg.col, wd);
+      if (P.dd) vstore<double, VEC>(P.dd + (size_t)i * ld + rg.col, wd);
       vstore<T, VEC>(P.d + (size_t)i * ld + rg.col, w);
     }
     reduce_cols_to_part<VEC>(acc, rg.G, ld, red, my_part);
@@ -79,7 +85,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
   {
     unsigned g0;
     if (grid_arrive(gs, g0)) {
-      reduce_partials(P.part, gridDim.x, ld, red, s_col[0]);
+      reduce_partials(P.part, vnb, ld, red, s_col[0]);
       int anyv = 0;
       for (int c = threadIdx.x; c < ld; c += blockDim.x) {
         const double rr = s_col[0][c];
@@ -128,7 +134,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
   bool capped = false;
   bool more = ld_volatile_i32(P.ctl + 3) != 0 && P.maxit > 0;
   if (ld_volatile_i32(P.ctl + 3) != 0 && P.maxit <= 0) capped = true;
-  const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+  const bool timer = vb == 0 && threadIdx.x == 0;
   uint64_t tmark = timer ? globaltimer_ns() : 0;
   auto lap = [&](int slot) {
     if (timer) {
@@ -145,17 +151,18 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
       first = false;
       pending = 0;
       flush_pending = false;
-      if (blockIdx.x == 0 && threadIdx.x == 0) P.stats[1] += 1;
+      if (vb == 0 && threadIdx.x == 0) P.stats[1] += 1;
     }
     lap(0);
     // ---- P1 ----
-    spmm_phase<T, VEC, WEIGHTED, true>(P.g, ld, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, red, P.act);
+    spmm_phase<T, VEC, WEIGHTED, true>(P.g, ld, shift0, P.d, P.v, ld, P.chunk_part, P.hcount, red, P.act, vb,
+                                       vnb);
     reduce_red_to_part(red, ld, my_part);
     // ---- R1 ----
     {
       unsigned g1;
       if (grid_arrive(gs, g1)) {
-        reduce_partials(P.part, gridDim.x, ld, red, s_col[0]);
+        reduce_partials(P.part, vnb, ld, red, s_col[0]);
         for (int c = threadIdx.x; c < ld; c += blockDim.x) {
           const int a_on = P.act[c];
           const double dv = s_col[0][c];
@@ -184,28 +191,31 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
         T* hslot = P.hist + (size_t)pending * nA * ld;
         constexpr int U = 2;
         for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
-          T rv[U][VEC], vv[U][VEC];
+          double rv[U][VEC];
+          T vv[U][VEC];
           long long ii[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const long long e = e0 + u * nth;
             ii[u] = e < nvec ? (e >> lgG) : -1;
             if (ii[u] >= 0) {
-              vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+              vload<double, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
               vload<T, VEC>(vv[u], P.v + (size_t)ii[u] * ld + rg.col);
             }
           }
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             if (ii[u] < 0) continue;
+            T rt[VEC];
 #pragma unroll
             for (int v = 0; v < VEC; ++v) {
-              if (on[v]) rv[u][v] = (T)((double)rv[u][v] - a_c[v] * (double)vv[u][v]);
-              racc[v] += (double)rv[u][v] * (double)rv[u][v];
+              if (on[v]) rv[u][v] = rv[u][v] - a_c[v] * (double)vv[u][v];
+              racc[v] += rv[u][v] * rv[u][v];
+              rt[v] = (T)rv[u][v];
             }
-            vstore<T, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
+            vstore<double, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
             const int ai = __ldg(P.active_pos + ii[u]);
-            if (ai >= 0) vstore<T, VEC>(hslot + (size_t)ai * ld + rg.col, rv[u]);
+            if (ai >= 0) vstore<T, VEC>(hslot + (size_t)ai * ld + rg.col, rt);
           }
         }
       }
@@ -216,7 +226,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
       unsigned g2;
       if (grid_arrive(gs, g2)) {
         double* s_rrn = s_col[0];
-        reduce_partials(P.part, gridDim.x, ld, red, s_rrn);
+        reduce_partials(P.part, vnb, ld, red, s_rrn);
         int anyv2 = 0;
         for (int c = threadIdx.x; c < ld; c += blockDim.x) {
           const int a_on = P.act[c];
@@ -299,15 +309,15 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
       if (any_on) {
         constexpr int U = 2;
         for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
-          T rv[U][VEC], dv[U][VEC];
+          double rv[U][VEC], dv[U][VEC];
           long long ii[U];
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const long long e = e0 + u * nth;
             ii[u] = e < nvec ? (e >> lgG) : -1;
             if (ii[u] >= 0) {
-              vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
-              vload<T, VEC>(dv[u], P.d + (size_t)ii[u] * ld + rg.col);
+              vload<double, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+              load_dir<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col);
             }
           }
 #pragma unroll
@@ -315,8 +325,8 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
             if (ii[u] < 0) continue;
 #pragma unroll
             for (int v = 0; v < VEC; ++v)
-              if (on[v]) dv[u][v] = (T)((double)rv[u][v] + be_c[v] * (double)dv[u][v]);
-            vstore<T, VEC>(P.d + (size_t)ii[u] * ld + rg.col, dv[u]);
+              if (on[v]) dv[u][v] = rv[u][v] + be_c[v] * dv[u][v];
+            store_dir<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col);
           }
         }
       }
@@ -330,7 +340,7 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
   // ---- final pass: remaining steps, X -> output ----
   shifted_update<T, E>(P, pending, first, true, tid, nth);
   lap(4);
-  if (blockIdx.x == 0) {
+  if (vb == 0) {
     if (P.track && P.h_out)
       for (int q = threadIdx.x; q < p * ld; q += blockDim.x) {
         const int j = q / ld, c = q % ld;
@@ -341,6 +351,34 @@ __global__ void __launch_bounds__(kBlock, 1) msolve_kernel(SolvePrm<T> P) {
       P.ctl[0] = capped ? (int)POLAR_ERR_ITER_CAP : 0;
     }
   }
+}
+
+template <typename T, int VEC, bool WEIGHTED, int E>
+__global__ void __launch_bounds__(kBlock, 1) msolve_kernel(const __grid_constant__ SolvePrm<T> P) {
+  msolve_run<T, VEC, WEIGHTED, E>(P, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// Many independent solves in one cooperative launch.  Problem b owns CTAs
+// [cta_off[b], cta_off[b+1]); its parameter block lives in its own workspace and is staged
+// in shared memory.  Problems never wait on one another: each share of CTAs runs its own
+// solve to convergence and leaves.
+constexpr int kMaxBatch = 64;
+struct BatchPrm {
+  int nprob;
+  int cta_off[kMaxBatch + 1];
+  const void* prm[kMaxBatch];
+};
+
+template <typename T, int VEC, bool WEIGHTED, int E>
+__global__ void __launch_bounds__(kBlock, 1) msolve_batch_kernel(const __grid_constant__ BatchPrm B) {
+  __shared__ __align__(16) int s_prm[(sizeof(SolvePrm<T>) + 3) / 4];
+  int b = 0;
+  while (b + 1 < B.nprob && (int)blockIdx.x >= B.cta_off[b + 1]) ++b;
+  const int* src = reinterpret_cast<const int*>(B.prm[b]);
+  for (int i = threadIdx.x; i < (int)(sizeof(SolvePrm<T>) / 4); i += blockDim.x) s_prm[i] = src[i];
+  __syncthreads();
+  const SolvePrm<T>& P = *reinterpret_cast<const SolvePrm<T>*>(s_prm);
+  msolve_run<T, VEC, WEIGHTED, E>(P, (int)blockIdx.x - B.cta_off[b], B.cta_off[b + 1] - B.cta_off[b]);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -378,7 +416,7 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
     L->off[k++] = o;
     o += align256(bytes);
   };
-  add(n * ld * ts);                                // 0 r
+  add(n * ld * 8);                                 // 0 r (FP64 in every precision)
   add(n * ld * ts);                                // 1 d
   add(n * ld * ts);                                // 2 v
   add((size_t)kHist * nA * ld * ts);               // 3 hist
@@ -400,6 +438,7 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
   add(4096);                                       // 30 device copy of the parameter block
   add((size_t)p * ld * kNC * 8);                   // 31 composed deferred-update coefficients
   add((size_t)kMaxHeavyCtas * ld * 8);             // 32 heavy-row d.v partials
+  add(precision == POLAR_MIXED ? n * ld * 8 : 0);  // 33 FP64 direction (mixed precision)
   L->total = o;
   L->ld = ld;
   L->vec = choose_vec(precision, ld);
@@ -492,6 +531,70 @@ extern "C" size_t polar_msolve_workspace_bytes(const polar_graph* g, int precisi
   return L.total;
 }
 
+// Parameter block of one solve: arguments as polar_msolve takes them, workspace regions
+// from the layout.  `composed`: deferred updates from composed coefficients (the
+// kernel-per-phase driver); the persistent kernels apply the per-step coefficients.
+template <typename TT>
+static void fill_prm(SolvePrm<TT>& prm, const polar_graph* g, int R, int ld, int p, int nA, double tol,
+                     int64_t maxit, int track, const double* d_W, int ldw, const double* d_tau,
+                     const int32_t* d_active, const int32_t* d_active_pos, void* d_X_out, int x_f32, int ldx,
+                     double* d_h_out, int64_t* d_iters_out, char* ws, const SolveLayout& L, bool composed) {
+  prm.g = *g;
+  prm.n = g->n;
+  prm.R = R;
+  prm.ld = ld;
+  prm.p = p;
+  prm.nA = nA;
+  prm.tol = tol;
+  prm.maxit = maxit;
+  prm.track = track;
+  prm.W = d_W;
+  prm.ldw = ldw;
+  prm.tau = d_tau;
+  prm.active = d_active;
+  prm.active_pos = d_active_pos;
+  prm.Xout = d_X_out;
+  prm.x_f32 = x_f32;
+  prm.ldx = ldx;
+  prm.h_out = d_h_out;
+  prm.iters_out = (long long*)d_iters_out;
+  prm.r = (double*)(ws + L.off[0]);
+  prm.d = (TT*)(ws + L.off[1]);
+  prm.v = (TT*)(ws + L.off[2]);
+  prm.hist = (TT*)(ws + L.off[3]);
+  prm.Pb = (TT*)(ws + L.off[4]);
+  prm.Xb = (TT*)(ws + L.off[5]);
+  prm.chunk_part = (TT*)(ws + L.off[6]);
+  prm.hcount = (int*)(ws + L.off[7]);
+  prm.part = (double*)(ws + L.off[8]);
+  prm.rr = (double*)(ws + L.off[9]);
+  prm.stop = (double*)(ws + L.off[10]);
+  prm.ap = (double*)(ws + L.off[11]);
+  prm.bp = (double*)(ws + L.off[12]);
+  prm.ag = (double*)(ws + L.off[13]);
+  prm.beg = (double*)(ws + L.off[14]);
+  prm.act = (int*)(ws + L.off[15]);
+  prm.upd = (int*)(ws + L.off[16]);
+  prm.z = (double*)(ws + L.off[17]);
+  prm.zp = (double*)(ws + L.off[18]);
+  prm.hs = (double*)(ws + L.off[19]);
+  prm.ip = (double*)(ws + L.off[20]);
+  prm.pn = (double*)(ws + L.off[21]);
+  prm.live = (int*)(ws + L.off[22]);
+  prm.pflag = (int*)(ws + L.off[23]);
+  prm.ca = (TT*)(ws + L.off[24]);
+  prm.cz = (TT*)(ws + L.off[25]);
+  prm.cb = (TT*)(ws + L.off[26]);
+  prm.ctl = (int*)(ws + L.off[27]);
+  prm.stats = (long long*)(ws + L.off[28]);
+  prm.chig = (double*)(ws + L.off[29]);
+  prm.cmp = composed ? (double*)(ws + L.off[31]) : nullptr;
+  prm.part_h = (double*)(ws + L.off[32]);
+  prm.dd = sizeof(TT) == 4 ? (double*)(ws + L.off[33]) : nullptr;
+  prm.nbh = 0;
+  prm.timeout_ns = g_timeout_ns;
+}
+
 extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d_W, int ldw, int R,
                             const double* d_tau, int p, const int32_t* d_active, const int32_t* d_active_pos,
                             int nA, double tol, int64_t maxit, int track, void* d_X_out, int x_f32, int ldx,
@@ -522,61 +625,8 @@ extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d
   if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync", e);
 
   auto fill = [&](auto* prm_ptr) {
-    auto& prm = *prm_ptr;
-    using TT = std::remove_pointer_t<decltype(prm.r)>;
-    prm.g = *g;
-    prm.n = g->n;
-    prm.R = R;
-    prm.ld = ld;
-    prm.p = p;
-    prm.nA = nA;
-    prm.tol = tol;
-    prm.maxit = maxit;
-    prm.track = track;
-    prm.W = d_W;
-    prm.ldw = ldw;
-    prm.tau = d_tau;
-    prm.active = d_active;
-    prm.active_pos = d_active_pos;
-    prm.Xout = d_X_out;
-    prm.x_f32 = x_f32;
-    prm.ldx = ldx;
-    prm.h_out = d_h_out;
-    prm.iters_out = (long long*)d_iters_out;
-    prm.r = (TT*)(ws + L.off[0]);
-    prm.d = (TT*)(ws + L.off[1]);
-    prm.v = (TT*)(ws + L.off[2]);
-    prm.hist = (TT*)(ws + L.off[3]);
-    prm.Pb = (TT*)(ws + L.off[4]);
-    prm.Xb = (TT*)(ws + L.off[5]);
-    prm.chunk_part = (TT*)(ws + L.off[6]);
-    prm.hcount = (int*)(ws + L.off[7]);
-    prm.part = (double*)(ws + L.off[8]);
-    prm.rr = (double*)(ws + L.off[9]);
-    prm.stop = (double*)(ws + L.off[10]);
-    prm.ap = (double*)(ws + L.off[11]);
-    prm.bp = (double*)(ws + L.off[12]);
-    prm.ag = (double*)(ws + L.off[13]);
-    prm.beg = (double*)(ws + L.off[14]);
-    prm.act = (int*)(ws + L.off[15]);
-    prm.upd = (int*)(ws + L.off[16]);
-    prm.z = (double*)(ws + L.off[17]);
-    prm.zp = (double*)(ws + L.off[18]);
-    prm.hs = (double*)(ws + L.off[19]);
-    prm.ip = (double*)(ws + L.off[20]);
-    prm.pn = (double*)(ws + L.off[21]);
-    prm.live = (int*)(ws + L.off[22]);
-    prm.pflag = (int*)(ws + L.off[23]);
-    prm.ca = (TT*)(ws + L.off[24]);
-    prm.cz = (TT*)(ws + L.off[25]);
-    prm.cb = (TT*)(ws + L.off[26]);
-    prm.ctl = (int*)(ws + L.off[27]);
-    prm.stats = (long long*)(ws + L.off[28]);
-    prm.chig = (double*)(ws + L.off[29]);
-    prm.cmp = g_solver_mode == 0 ? (double*)(ws + L.off[31]) : nullptr;
-    prm.part_h = (double*)(ws + L.off[32]);
-    prm.nbh = 0;
-    prm.timeout_ns = g_timeout_ns;
+    fill_prm(*prm_ptr, g, R, ld, p, nA, tol, maxit, track, d_W, ldw, d_tau, d_active, d_active_pos, d_X_out, x_f32,
+             ldx, d_h_out, d_iters_out, ws, L, g_solver_mode == 0);
   };
   int rc;
   if (g_solver_mode == 0) {
@@ -659,4 +709,242 @@ extern "C" int polar_msolve_finish(void* d_workspace, polar_stream_t stream, pol
   if (status == POLAR_ERR_NONFINITE) return set_error(status, "non-finite value in CG");
   if (status == POLAR_ERR_TIMEOUT) return set_error(status, "grid barrier wait timed out");
   return status;
+}
+
+// ---------------------------------------------------------------------------------------
+// Batched solves: many graphs (or many right-hand-side blocks) in one cooperative launch
+// of the persistent kernel, the CTAs split between the problems in proportion to their
+// work.
+namespace polar {
+
+static_assert(sizeof(SolvePrm<double>) <= 4096 && sizeof(SolvePrm<float>) <= 4096,
+              "parameter block must fit its workspace region");
+
+template <typename T, int VEC, bool WEIGHTED, int E>
+static int batch_occupancy() {
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, msolve_batch_kernel<T, VEC, WEIGHTED, E>, kBlock, 0);
+  return nb;
+}
+
+static int batch_grid_max(int precision, int vec, bool weighted) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int nb = 0;
+  if (precision == POLAR_MIXED) {
+    if (vec == 4) nb = weighted ? batch_occupancy<float, 4, true, POLAR_E32>() : batch_occupancy<float, 4, false, POLAR_E32>();
+    else if (vec == 2) nb = weighted ? batch_occupancy<float, 2, true, POLAR_E32>() : batch_occupancy<float, 2, false, POLAR_E32>();
+    else nb = weighted ? batch_occupancy<float, 1, true, POLAR_E32>() : batch_occupancy<float, 1, false, POLAR_E32>();
+  } else {
+    if (vec == 2) nb = weighted ? batch_occupancy<double, 2, true, POLAR_E64>() : batch_occupancy<double, 2, false, POLAR_E64>();
+    else nb = weighted ? batch_occupancy<double, 1, true, POLAR_E64>() : batch_occupancy<double, 1, false, POLAR_E64>();
+  }
+  if (nb < 1) nb = 1;
+  return nb * sms;
+}
+
+template <typename T, int VEC, bool WEIGHTED, int E>
+static int launch_batch(const BatchPrm& B, int grid, cudaStream_t st) {
+  void* args[] = {(void*)&B};
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)msolve_batch_kernel<T, VEC, WEIGHTED, E>, dim3(grid),
+                                              dim3(kBlock), args, 0, st);
+  count_launch();
+  if (e != cudaSuccess) return set_cuda_error("cudaLaunchCooperativeKernel(msolve batch)", e);
+  return POLAR_OK;
+}
+
+// CTA split: one CTA per problem, the rest in proportion to cost (largest remainders),
+// each problem capped where its row streams would give a thread fewer than two items.
+static void split_ctas(const std::vector<double>& cost, const std::vector<int>& cap, int total,
+                       std::vector<int>& ctas) {
+  const int np = (int)cost.size();
+  ctas.assign(np, 1);
+  int left = total - np;
+  double csum = 0.0;
+  for (double c : cost) csum += c;
+  if (left <= 0 || csum <= 0.0) return;
+  std::vector<double> frac(np, 0.0);
+  int used = 0;
+  for (int b = 0; b < np; ++b) {
+    const double want = left * cost[b] / csum;
+    int add = (int)want;
+    if (ctas[b] + add > cap[b]) add = cap[b] - ctas[b] > 0 ? cap[b] - ctas[b] : 0;
+    ctas[b] += add;
+    used += add;
+    frac[b] = want - (double)(int)want;
+  }
+  left -= used;
+  // hand out the rest one at a time: largest remainder first, then any problem below its cap
+  while (left > 0) {
+    int best = -1;
+    for (int b = 0; b < np; ++b)
+      if (ctas[b] < cap[b] && (best < 0 || frac[b] > frac[best])) best = b;
+    if (best < 0) break;
+    ctas[best] += 1;
+    frac[best] = -1.0;
+    --left;
+    bool any = false;
+    for (int b = 0; b < np; ++b) any |= frac[b] >= 0.0 && ctas[b] < cap[b];
+    if (!any)
+      for (int b = 0; b < np; ++b) frac[b] = cost[b];
+  }
+}
+
+}  // namespace polar
+
+// Kernel-per-phase driver for a batch: every problem's solve on its own stream with its
+// grids scaled to its rows (a problem too small to fill the GPU takes a share of it), the
+// host relaunching each solve's iteration block as soon as the previous one drains.
+template <typename T, int VEC, bool W, int E>
+static int batch_graph_run(const polar_msolve_problem* probs, int nprob, int ld, const std::vector<SolveLayout>& L,
+                           cudaStream_t st) {
+  std::vector<SolvePrm<T>> prm(nprob);
+  std::vector<double> frac(nprob);
+  const int full = mk_grid_max<T, VEC, W, E>();
+  for (int b = 0; b < nprob; ++b) {
+    const polar_msolve_problem& q = probs[b];
+    char* ws = (char*)q.d_workspace;
+    cudaError_t e = cudaMemsetAsync(ws + L[b].off[27], 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws + L[b].off[28], 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws + L[b].off[7], 0, L[b].off[8] - L[b].off[7], st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(q.d_iters_out, 0, sizeof(int64_t) * q.R, st);
+    if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync (batch)", e);
+    fill_prm(prm[b], q.g, q.R, ld, q.p, q.nA, q.tol, q.maxit, q.track, q.d_W, q.ldw, q.d_tau, q.d_active,
+             q.d_active_pos, q.d_X_out, q.x_f32, q.ldx, q.d_h_out, q.d_iters_out, ws, L[b], true);
+    // two row items per thread of the full grid count as a full share
+    const double items = (double)q.g->n * (ld / VEC);
+    const double f = items / ((double)full * kBlock * 2.0);
+    frac[b] = f < 1.0 ? f : 1.0;
+  }
+  std::vector<MkResult> res;
+  const int rc = mk_solve_batch<T, VEC, W, E>(prm, frac, st, res);
+  if (rc != POLAR_OK) return rc;
+  for (int b = 0; b < nprob; ++b) {
+    const int status = res[b].err ? res[b].err : (res[b].capped ? (int)POLAR_ERR_ITER_CAP : 0);
+    remember_solve_done(probs[b].d_workspace, status, res[b].iterations, res[b].flushes, ld, res[b].grid, kBlock);
+  }
+  return POLAR_OK;
+}
+
+static int batch_graph_driver(const polar_msolve_problem* probs, int nprob, int precision, int ld, int vec,
+                              bool weighted, const std::vector<SolveLayout>& L, cudaStream_t st) {
+  if (precision == POLAR_MIXED) {
+    if (vec == 4) return weighted ? batch_graph_run<float, 4, true, POLAR_E32>(probs, nprob, ld, L, st)
+                                  : batch_graph_run<float, 4, false, POLAR_E32>(probs, nprob, ld, L, st);
+    if (vec == 2) return weighted ? batch_graph_run<float, 2, true, POLAR_E32>(probs, nprob, ld, L, st)
+                                  : batch_graph_run<float, 2, false, POLAR_E32>(probs, nprob, ld, L, st);
+    return weighted ? batch_graph_run<float, 1, true, POLAR_E32>(probs, nprob, ld, L, st)
+                    : batch_graph_run<float, 1, false, POLAR_E32>(probs, nprob, ld, L, st);
+  }
+  if (vec == 2) return weighted ? batch_graph_run<double, 2, true, POLAR_E64>(probs, nprob, ld, L, st)
+                                : batch_graph_run<double, 2, false, POLAR_E64>(probs, nprob, ld, L, st);
+  return weighted ? batch_graph_run<double, 1, true, POLAR_E64>(probs, nprob, ld, L, st)
+                  : batch_graph_run<double, 1, false, POLAR_E64>(probs, nprob, ld, L, st);
+}
+
+static int batch_layout_grid(int precision, int vec, bool weighted) {
+  return g_solver_mode == 0 ? grid_for_mode(precision, vec, weighted) : batch_grid_max(precision, vec, weighted);
+}
+
+extern "C" size_t polar_msolve_batch_workspace_bytes(const polar_graph* g, int precision, int R, int p, int nA) {
+  if (!g || R < 1 || p < 1 || nA < 0) return 0;
+  const int ld = choose_ld(precision, R);
+  SolveLayout L;
+  solve_layout(g, precision, R, p, nA, batch_layout_grid(precision, choose_vec(precision, ld), g->d_wts != nullptr),
+               &L);
+  return L.total;
+}
+
+extern "C" int polar_msolve_batch(const polar_msolve_problem* probs, int nprob, int precision,
+                                  polar_stream_t stream) {
+  clear_error();
+  if (!probs || nprob < 1) return set_error(POLAR_ERR_BAD_ARG, "no problems");
+  if (nprob > kMaxBatch) return set_error(POLAR_ERR_BAD_ARG, "at most 64 problems per batch");
+  if (precision != POLAR_FP64 && precision != POLAR_MIXED) return set_error(POLAR_ERR_BAD_ARG, "precision");
+  const int ld = choose_ld(precision, probs[0].R);
+  const bool weighted = probs[0].g && probs[0].g->d_wts != nullptr;
+  for (int b = 0; b < nprob; ++b) {
+    const polar_msolve_problem& q = probs[b];
+    const polar_graph* g = q.g;
+    if (!g || !q.d_W || !q.d_tau || !q.d_active || !q.d_active_pos || !q.d_X_out || !q.d_iters_out || !q.d_workspace)
+      return set_error(POLAR_ERR_BAD_ARG, "null pointer in a batch problem");
+    if (q.R < 1 || q.R > max_ld(precision)) return set_error(POLAR_ERR_BAD_ARG, "R out of range for this precision");
+    if (q.p < 1 || q.nA < 1 || q.ldw < q.R || q.ldx < q.R || g->n < 1)
+      return set_error(POLAR_ERR_BAD_ARG, "bad sizes in a batch problem");
+    if (q.track && !q.d_h_out) return set_error(POLAR_ERR_BAD_ARG, "track needs h_out");
+    if ((g->d_wts == nullptr) != (g->d_diag == nullptr)) return set_error(POLAR_ERR_BAD_ARG, "weights and diag go together");
+    if (choose_ld(precision, q.R) != ld) return set_error(POLAR_ERR_BAD_ARG, "batch problems must share the padded width");
+    if ((g->d_wts != nullptr) != weighted) return set_error(POLAR_ERR_BAD_ARG, "batch problems must all be weighted or all unweighted");
+  }
+  const int vec = choose_vec(precision, ld);
+  const int gmax = batch_layout_grid(precision, vec, weighted);
+  if (g_solver_mode != 0 && nprob > gmax) return set_error(POLAR_ERR_BAD_ARG, "more problems than co-resident CTAs");
+  std::vector<SolveLayout> L(nprob);
+  std::vector<double> cost(nprob);
+  std::vector<int> cap(nprob), ctas;
+  for (int b = 0; b < nprob; ++b) {
+    const polar_msolve_problem& q = probs[b];
+    solve_layout(q.g, precision, q.R, q.p, q.nA, gmax, &L[b]);
+    if (q.workspace_bytes < L[b].total) return set_error(POLAR_ERR_WORKSPACE, "workspace too small (batch problem)");
+    const double n = q.g->n, nnz = q.g->nnz;
+    cost[b] = q.cost > 0.0 ? q.cost : (nnz + 2.0 * n) * ld / sqrt(q.g->sigma > 0.0 ? q.g->sigma : 1.0);
+    const long long items = (long long)q.g->n * (ld / vec);
+    long long c = (items + 2LL * kBlock - 1) / (2LL * kBlock);
+    cap[b] = (int)(c < 1 ? 1 : (c > gmax ? gmax : c));
+  }
+  // each problem's barrier words and scratch live in its own workspace: no sharing
+  for (int b = 0; b < nprob; ++b)
+    for (int c = b + 1; c < nprob; ++c) {
+      const char* b0 = (const char*)probs[b].d_workspace;
+      const char* c0 = (const char*)probs[c].d_workspace;
+      if (b0 < c0 + L[c].total && c0 < b0 + L[b].total)
+        return set_error(POLAR_ERR_BAD_ARG, "batch problems must not share workspace memory");
+    }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (g_solver_mode == 0) return batch_graph_driver(probs, nprob, precision, ld, vec, weighted, L, st);
+  split_ctas(cost, cap, gmax, ctas);
+  BatchPrm B;
+  memset(&B, 0, sizeof(B));
+  B.nprob = nprob;
+  B.cta_off[0] = 0;
+  for (int b = 0; b < nprob; ++b) B.cta_off[b + 1] = B.cta_off[b] + ctas[b];
+  const int grid = B.cta_off[nprob];
+  for (int b = 0; b < nprob; ++b) {
+    const polar_msolve_problem& q = probs[b];
+    char* ws = (char*)q.d_workspace;
+    cudaError_t e = cudaMemsetAsync(ws + L[b].off[27], 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws + L[b].off[28], 0, 64, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws + L[b].off[7], 0, L[b].off[8] - L[b].off[7], st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(q.d_iters_out, 0, sizeof(int64_t) * q.R, st);
+    if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync (batch)", e);
+    if (precision == POLAR_MIXED) {
+      SolvePrm<float> prm;
+      fill_prm(prm, q.g, q.R, ld, q.p, q.nA, q.tol, q.maxit, q.track, q.d_W, q.ldw, q.d_tau, q.d_active,
+               q.d_active_pos, q.d_X_out, q.x_f32, q.ldx, q.d_h_out, q.d_iters_out, ws, L[b], false);
+      e = cudaMemcpyAsync(ws + L[b].off[30], &prm, sizeof(prm), cudaMemcpyHostToDevice, st);
+    } else {
+      SolvePrm<double> prm;
+      fill_prm(prm, q.g, q.R, ld, q.p, q.nA, q.tol, q.maxit, q.track, q.d_W, q.ldw, q.d_tau, q.d_active,
+               q.d_active_pos, q.d_X_out, q.x_f32, q.ldx, q.d_h_out, q.d_iters_out, ws, L[b], false);
+      e = cudaMemcpyAsync(ws + L[b].off[30], &prm, sizeof(prm), cudaMemcpyHostToDevice, st);
+    }
+    if (e != cudaSuccess) return set_cuda_error("parameter block upload (batch)", e);
+    B.prm[b] = ws + L[b].off[30];
+  }
+  int rc;
+  if (precision == POLAR_MIXED) {
+    if (vec == 4) rc = weighted ? launch_batch<float, 4, true, POLAR_E32>(B, grid, st) : launch_batch<float, 4, false, POLAR_E32>(B, grid, st);
+    else if (vec == 2) rc = weighted ? launch_batch<float, 2, true, POLAR_E32>(B, grid, st) : launch_batch<float, 2, false, POLAR_E32>(B, grid, st);
+    else rc = weighted ? launch_batch<float, 1, true, POLAR_E32>(B, grid, st) : launch_batch<float, 1, false, POLAR_E32>(B, grid, st);
+  } else {
+    if (vec == 2) rc = weighted ? launch_batch<double, 2, true, POLAR_E64>(B, grid, st) : launch_batch<double, 2, false, POLAR_E64>(B, grid, st);
+    else rc = weighted ? launch_batch<double, 1, true, POLAR_E64>(B, grid, st) : launch_batch<double, 1, false, POLAR_E64>(B, grid, st);
+  }
+  if (rc != POLAR_OK) return rc;
+  for (int b = 0; b < nprob; ++b) {
+    char* ws = (char*)probs[b].d_workspace;
+    remember_solve(probs[b].d_workspace, (int*)(ws + L[b].off[27]), (long long*)(ws + L[b].off[28]), ld, ctas[b], kBlock);
+  }
+  return POLAR_OK;
 }

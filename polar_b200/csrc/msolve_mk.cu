@@ -20,6 +20,7 @@
 #include <map>
 #include <vector>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <type_traits>
 
@@ -74,14 +75,17 @@ __global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolveP
   for (int v = 0; v < VEC; ++v) acc[v] = 0.0;
   for (long long e = tid; e < nvec; e += nth) {
     const long long i = e >> lgG;
+    double wd[VEC];
     T w[VEC];
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
       const int c = rg.col + v;
-      w[v] = (c < P.R) ? (T)__ldg(P.W + (size_t)i * P.ldw + c) : T(0);
-      acc[v] += (double)w[v] * (double)w[v];
+      wd[v] = (c < P.R) ? __ldg(P.W + (size_t)i * P.ldw + c) : 0.0;
+      w[v] = (T)wd[v];
+      acc[v] += wd[v] * wd[v];
     }
-    vstore<T, VEC>(P.r + (size_t)i * ld + rg.col, w);
+    vstore<double, VEC>(P.r + (size_t)i * ld + rg.col, wd);
+    if (P.dd) vstore<double, VEC>(P.dd + (size_t)i * ld + rg.col, wd);
     vstore<T, VEC>(P.d + (size_t)i * ld + rg.col, w);
   }
   reduce_cols_to_part<VEC>(acc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
@@ -466,7 +470,8 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
     T* hslot = P.hist + (size_t)slot * nA * ld;
     constexpr int U = POLAR_RESID_U;
     for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
-      T rv[U][VEC], vv[U][VEC];
+      double rv[U][VEC];
+      T vv[U][VEC];
       long long ii[U];
       int ai[U];
 #pragma unroll
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
         const long long e = e0 + u * nth;
         ii[u] = e < nvec ? (e >> lgG) : -1;
         if (ii[u] >= 0) {
-          vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+          vload<double, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
           vload<T, VEC>(vv[u], P.v + (size_t)ii[u] * ld + rg.col);
           ai[u] = __ldg(P.active_pos + ii[u]);
         }
@@ -482,13 +487,15 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (ii[u] < 0) continue;
+        T rt[VEC];
 #pragma unroll
         for (int v = 0; v < VEC; ++v) {
-          if (on[v]) rv[u][v] = (T)((double)rv[u][v] - a_c[v] * (double)vv[u][v]);
-          racc[v] += (double)rv[u][v] * (double)rv[u][v];
+          if (on[v]) rv[u][v] = rv[u][v] - a_c[v] * (double)vv[u][v];
+          racc[v] += rv[u][v] * rv[u][v];
+          rt[v] = (T)rv[u][v];
         }
-        vstore<T, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
-        if (ai[u] >= 0) vstore_cs<T, VEC>(hslot + (size_t)ai[u] * ld + rg.col, rv[u]);
+        vstore<double, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
+        if (ai[u] >= 0) vstore_cs<T, VEC>(hslot + (size_t)ai[u] * ld + rg.col, rt);
       }
     }
   }
@@ -539,17 +546,18 @@ __global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ Solv
       any_on |= on[v];
     }
     if (any_on) {
-      constexpr int U = POLAR_STREAM_U;
+      // FP64 r doubles the registers of a row item: fewer items in flight for wide FP32 rows
+      constexpr int U = (sizeof(T) == 4 && VEC >= 4 && POLAR_STREAM_U > 2) ? 2 : POLAR_STREAM_U;
       for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
-        T rv[U][VEC], dv[U][VEC];
+        double rv[U][VEC], dv[U][VEC];
         long long ii[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const long long e = e0 + u * nth;
           ii[u] = e < nvec ? (e >> lgG) : -1;
           if (ii[u] >= 0) {
-            vload<T, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
-            vload<T, VEC>(dv[u], P.d + (size_t)ii[u] * ld + rg.col);
+            vload<double, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+            load_dir<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col);
           }
         }
 #pragma unroll
@@ -557,8 +565,8 @@ __global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ Solv
           if (ii[u] < 0) continue;
 #pragma unroll
           for (int v = 0; v < VEC; ++v)
-            if (on[v]) dv[u][v] = (T)((double)rv[u][v] + be_c[v] * (double)dv[u][v]);
-          vstore<T, VEC>(P.d + (size_t)ii[u] * ld + rg.col, dv[u]);
+            if (on[v]) dv[u][v] = rv[u][v] + be_c[v] * dv[u][v];
+          store_dir<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col);
         }
       }
     }
@@ -775,110 +783,133 @@ static void timed(int cls, double bytes, cudaStream_t st, F&& launch) {
   timing_push(t);
 }
 
+// One solve of the kernel-per-phase driver as a restartable object: start() clears the
+// history, launches the initialisation and captures the iteration block (M iterations and
+// one deferred-update pass) as a CUDA graph; launch() queues one block on the solve's
+// stream; check() (after that stream has drained the block) reads the control words and
+// decides whether the solve is done.  mk_solve runs one object to completion; the batched
+// driver keeps one per problem, each on its own stream, so small solves overlap.
+// grid_frac in (0, 1] scales every grid (the kernels stride over any grid), so that
+// concurrent solves share the SMs.
 template <typename T, int VEC, bool W, int E>
-int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
-  SolvePrm<T> P = P0;
-  // heavy chunks run in their own launch when there are any (one warp per chunk, at most
-  // two CTAs per SM), except on the sliced-ELL path, whose launch takes them first
-  {
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int want = (P.g.nchunks + kWarps - 1) / kWarps;
-    const int cap = 2 * sms;
-    P.nbh = P.g.nchunks > 0 ? (want < cap ? want : cap) : 0;
-    if (P.nbh > kMaxHeavyCtas) P.nbh = kMaxHeavyCtas;
-  }
-  (void)dev_prm;
-  const double s = sizeof(T), n = P.n, R = P.R, nA = P.nA;
-  // algorithmic bytes per launch (unweighted CSR: values implicit, diagonal from indptr)
-  const double b_spmm = 4.0 * (n + 1) + 4.0 * P.g.nnz + 2.0 * s * n * R;
-  const double b_resid = 3.0 * s * n * R + s * nA * R;
-  const double b_dir = 3.0 * s * n * R;
-  const double b_flush = (4.0 * P.p + kHist) * s * nA * R;
-  const int g0 = occ_grid(mk_init<T, VEC>, kBlock);
-  const int cpl = spmm_cpl<T>(P.ld, VEC);
-  if (spmm_merged<T, W>(cpl, P)) P.nbh = 0;
-  const int g1 = spmm_grid<T, W>(cpl);
-  const int g3 = occ_grid(mk_resid<T, VEC>, kBlock);
-  const int g4 = occ_grid(mk_dir<T, VEC>, kBlock);
-  const size_t s5 = flush_smem_for<T, E>(P);
-  const int g5 = flush_grid<T, E>(P, s5);
-  // the composed flush multiplies every history slot (zero coefficients for unused ones)
-  cudaError_t e = cudaMemsetAsync(P.hist, 0, sizeof(T) * (size_t)kHist * P.nA * P.ld, st);
-  if (e != cudaSuccess) return set_cuda_error("history clear", e);
-  timed(KC_INIT, 2.0 * s * n * R + 8.0 * n * R, st, [&] { mk_init<T, VEC><<<g0, kBlock, 0, st>>>(P); });
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return set_cuda_error("mk_init", e);
-  // One block = M iterations and one deferred-update pass, captured once per solve as a
-  // CUDA graph (the parameters are fixed for the whole solve) and launched until
-  // convergence.  With kernel timing on, each kernel node is bracketed by event nodes.
-  const bool timing = timing_on();
+struct MkSolver {
   struct GraphTimed {
     int cls;
     double bytes;
     cudaEvent_t a, b;
   };
-  std::vector<GraphTimed> gt;
-  auto node = [&](cudaStream_t cs, int cls, double bytes, auto&& launch) {
-    if (timing) {
-      GraphTimed t{cls, bytes, nullptr, nullptr};
-      cudaEventCreate(&t.a);
-      cudaEventCreate(&t.b);
-      // inside capture only an external record becomes an event-record node
-      cudaEventRecordWithFlags(t.a, cs, cudaEventRecordExternal);
-      launch(cs);
-      cudaEventRecordWithFlags(t.b, cs, cudaEventRecordExternal);
-      gt.push_back(t);
-    } else {
-      launch(cs);
-    }
-  };
-  cudaStream_t cs;
-  e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return set_cuda_error("capture stream", e);
-  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-  if (e != cudaSuccess) {
-    cudaStreamDestroy(cs);
-    return set_cuda_error("begin capture", e);
-  }
-  for (int k = 0; k < kHist; ++k) {
-    if (P.nbh > 0) node(cs, KC_HEAVY, 0.0, [&](cudaStream_t x) { spmm_go<T, W>(1, cpl, g1, P, x); });
-    node(cs, KC_SPMM, b_spmm, [&](cudaStream_t x) { spmm_go<T, W>(2, cpl, g1, P, x); });
-    node(cs, KC_RESID, b_resid, [&](cudaStream_t x) { launch_k(mk_resid<T, VEC>, g3, kBlock, 0, x, P, k); });
-    node(cs, KC_DIR, b_dir, [&](cudaStream_t x) { launch_k(mk_dir<T, VEC>, g4, kBlock, 0, x, P, k); });
-  }
-  node(cs, KC_FLUSH, b_flush, [&](cudaStream_t x) { launch_k(mk_flush<T, E>, g5, kBlock, s5, x, P, 0); });
+  SolvePrm<T> P;
+  cudaStream_t st = nullptr;
+  cudaStream_t cs = nullptr;
   cudaGraph_t graph = nullptr;
-  e = cudaStreamEndCapture(cs, &graph);
   cudaGraphExec_t exec = nullptr;
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  auto cleanup = [&]() {
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    cudaStreamDestroy(cs);
-    for (auto& t : gt) {
-      cudaEventDestroy(t.a);
-      cudaEventDestroy(t.b);
-    }
-  };
-  if (e != cudaSuccess) {
-    cleanup();
-    return set_cuda_error("graph build", e);
+  std::vector<GraphTimed> gt;
+  bool timing = false;
+  int g5 = 1, per_block = 0;
+  size_t s5 = 0;
+  double b_flush = 0.0;
+  int ctl[8] = {0};
+  long long stats[2] = {0, 0};
+  bool done = false;
+  MkResult res{};
+
+  static int scaled(int g, double f, int mult) {
+    int x = (int)(g * f + 0.5);
+    if (x < mult) x = mult;
+    x -= x % mult;
+    return x < mult ? mult : x;
   }
-  const int per_block = (P.nbh > 0 ? 4 : 3) * kHist + 1;
-  int ctl[8];
-  long long stats[2];
-  for (;;) {
-    e = cudaGraphLaunch(exec, st);
+
+  int start(const SolvePrm<T>& P0, cudaStream_t stream, double grid_frac) {
+    P = P0;
+    st = stream;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const double f = grid_frac > 0.0 && grid_frac < 1.0 ? grid_frac : 1.0;
+    // heavy chunks run in their own launch when there are any (one warp per chunk, at most
+    // two CTAs per SM), except on the sliced-ELL path, whose launch takes them first
+    {
+      const int want = (P.g.nchunks + kWarps - 1) / kWarps;
+      const int cap = scaled(2 * sms, f, 1);
+      P.nbh = P.g.nchunks > 0 ? (want < cap ? want : cap) : 0;
+      if (P.nbh > kMaxHeavyCtas) P.nbh = kMaxHeavyCtas;
+    }
+    const double s = sizeof(T), n = P.n, R = P.R, nA = P.nA;
+    // algorithmic bytes per launch (unweighted CSR: values implicit, diagonal from indptr)
+    const double b_spmm = 4.0 * (n + 1) + 4.0 * P.g.nnz + 2.0 * s * n * R;
+    // r is FP64 in both precisions; mixed precision keeps an FP64 direction beside d
+    const double b_resid = (16.0 + s) * n * R + s * nA * R;
+    const double b_dir = (s == 4.0 ? 28.0 : 24.0) * n * R;  // mixed: r, dd in; dd, d out
+    b_flush = (4.0 * P.p + kHist) * s * nA * R;
+    const int g0 = scaled(occ_grid(mk_init<T, VEC>, kBlock), f, 1);
+    const int cpl = spmm_cpl<T>(P.ld, VEC);
+    if (spmm_merged<T, W>(cpl, P)) P.nbh = 0;
+    const int g1 = scaled(spmm_grid<T, W>(cpl), f, 1);
+    const int g3 = scaled(occ_grid(mk_resid<T, VEC>, kBlock), f, 1);
+    const int g4 = scaled(occ_grid(mk_dir<T, VEC>, kBlock), f, 1);
+    s5 = flush_smem_for<T, E>(P);
+    g5 = scaled(flush_grid<T, E>(P, s5), f, P.ld / flush_cw<T>(P.ld));
+    res.grid = g1;
+    // the composed flush multiplies every history slot (zero coefficients for unused ones)
+    cudaError_t e = cudaMemsetAsync(P.hist, 0, sizeof(T) * (size_t)kHist * P.nA * P.ld, st);
+    if (e != cudaSuccess) return set_cuda_error("history clear", e);
+    timed(KC_INIT, (16.0 + s) * n * R, st, [&] { mk_init<T, VEC><<<g0, kBlock, 0, st>>>(P); });
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error("mk_init", e);
+    // One block = M iterations and one deferred-update pass, captured once per solve as a
+    // CUDA graph (the parameters are fixed for the whole solve) and launched until
+    // convergence.  With kernel timing on, each kernel node is bracketed by event nodes.
+    timing = timing_on();
+    auto node = [&](cudaStream_t x, int cls, double bytes, auto&& launch) {
+      if (timing) {
+        GraphTimed t{cls, bytes, nullptr, nullptr};
+        cudaEventCreate(&t.a);
+        cudaEventCreate(&t.b);
+        // inside capture only an external record becomes an event-record node
+        cudaEventRecordWithFlags(t.a, x, cudaEventRecordExternal);
+        launch(x);
+        cudaEventRecordWithFlags(t.b, x, cudaEventRecordExternal);
+        gt.push_back(t);
+      } else {
+        launch(x);
+      }
+    };
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      cs = nullptr;
+      return set_cuda_error("capture stream", e);
+    }
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return set_cuda_error("begin capture", e);
+    for (int k = 0; k < kHist; ++k) {
+      if (P.nbh > 0) node(cs, KC_HEAVY, 0.0, [&](cudaStream_t x) { spmm_go<T, W>(1, cpl, g1, P, x); });
+      node(cs, KC_SPMM, b_spmm, [&](cudaStream_t x) { spmm_go<T, W>(2, cpl, g1, P, x); });
+      node(cs, KC_RESID, b_resid, [&](cudaStream_t x) { launch_k(mk_resid<T, VEC>, g3, kBlock, 0, x, P, k); });
+      node(cs, KC_DIR, b_dir, [&](cudaStream_t x) { launch_k(mk_dir<T, VEC>, g4, kBlock, 0, x, P, k); });
+    }
+    node(cs, KC_FLUSH, b_flush, [&](cudaStream_t x) { launch_k(mk_flush<T, E>, g5, kBlock, s5, x, P, 0); });
+    e = cudaStreamEndCapture(cs, &graph);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) return set_cuda_error("graph build", e);
+    per_block = (P.nbh > 0 ? 4 : 3) * kHist + 1;
+    return POLAR_OK;
+  }
+
+  int launch() {
+    cudaError_t e = cudaGraphLaunch(exec, st);
     count_launch(per_block);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return set_cuda_error("msolve block", e);
+    return POLAR_OK;
+  }
+
+  // Reads the control words once the stream has executed the last launched block (the
+  // copies are ordered after it).  Sets `done` and fills `res`.
+  int check() {
+    cudaError_t e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-      cleanup();
-      return set_cuda_error("msolve block", e);
-    }
+    if (e != cudaSuccess) return set_cuda_error("msolve block", e);
     if (timing)
       for (auto& t : gt) {
         float ms = 0.f;
@@ -887,27 +918,129 @@ int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkRes
         else
           cudaGetLastError();
       }
-    if (ctl[C_ERR] != 0 || ctl[C_ANY] == 0) break;
-    if (stats[0] >= P.maxit) {
+    if (ctl[C_ERR] != 0 || ctl[C_ANY] == 0) {
+      done = true;
+    } else if (stats[0] >= P.maxit) {
       timed(KC_FLUSH, b_flush, st, [&] { mk_flush<T, E><<<g5, kBlock, s5, st>>>(P, 1); });
       e = cudaMemcpyAsync(ctl, P.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaMemcpyAsync(stats, P.stats, sizeof(stats), cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e != cudaSuccess) {
-        cleanup();
-        return set_cuda_error("msolve sync", e);
-      }
+      if (e != cudaSuccess) return set_cuda_error("msolve sync", e);
+      done = true;
+    }
+    if (done) {
+      res.err = ctl[C_ERR];
+      res.capped = ctl[C_ERR] == 0 && ctl[C_ANY] != 0;
+      res.iterations = stats[0];
+      res.flushes = stats[1];
+    }
+    return POLAR_OK;
+  }
+
+  void cleanup() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cs) cudaStreamDestroy(cs);
+    for (auto& t : gt) {
+      cudaEventDestroy(t.a);
+      cudaEventDestroy(t.b);
+    }
+    exec = nullptr;
+    graph = nullptr;
+    cs = nullptr;
+    gt.clear();
+  }
+};
+
+template <typename T, int VEC, bool W, int E>
+int mk_solve(const SolvePrm<T>& P0, SolvePrm<T>* dev_prm, cudaStream_t st, MkResult* out) {
+  (void)dev_prm;
+  MkSolver<T, VEC, W, E> S;
+  int rc = S.start(P0, st, 1.0);
+  while (rc == POLAR_OK && !S.done) {
+    rc = S.launch();
+    if (rc == POLAR_OK) rc = S.check();
+  }
+  if (S.timing) timing_collect();
+  S.cleanup();
+  if (rc != POLAR_OK) return rc;
+  *out = S.res;
+  return POLAR_OK;
+}
+
+// Many solves at once: one MkSolver per problem, each on its own stream (ordered after
+// the caller's stream) with grids scaled by its share of the work.  The host polls the
+// streams and relaunches each solve's block as soon as its previous one has drained, so
+// a short solve never waits for a long one.
+template <typename T, int VEC, bool W, int E>
+int mk_solve_batch(const std::vector<SolvePrm<T>>& Ps, const std::vector<double>& frac, cudaStream_t st,
+                   std::vector<MkResult>& out) {
+  const int np = (int)Ps.size();
+  std::vector<MkSolver<T, VEC, W, E>> S(np);
+  std::vector<cudaStream_t> ss(np, nullptr);
+  std::vector<cudaEvent_t> ev(np, nullptr);
+  cudaEvent_t ready = nullptr;
+  int rc = POLAR_OK;
+  cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(ready, st);
+  if (e != cudaSuccess) rc = set_cuda_error("batch start event", e);
+  for (int b = 0; b < np && rc == POLAR_OK; ++b) {
+    e = cudaStreamCreateWithFlags(&ss[b], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ss[b], ready, 0);
+    if (e != cudaSuccess) {
+      rc = set_cuda_error("batch stream", e);
       break;
     }
+    rc = S[b].start(Ps[b], ss[b], frac[b]);
   }
-  if (timing) timing_collect();
-  cleanup();
-  out->err = ctl[C_ERR];
-  out->capped = ctl[C_ERR] == 0 && ctl[C_ANY] != 0;
-  out->iterations = stats[0];
-  out->flushes = stats[1];
-  out->grid = g1;
-  return POLAR_OK;
+  std::vector<char> queued(np, 0);
+  for (int b = 0; b < np && rc == POLAR_OK; ++b) {
+    rc = S[b].launch();
+    if (rc == POLAR_OK && cudaEventRecord(ev[b], ss[b]) != cudaSuccess) rc = set_cuda_error("batch event", cudaGetLastError());
+    queued[b] = 1;
+  }
+  int live = np;
+  while (rc == POLAR_OK && live > 0) {
+    bool progressed = false;
+    for (int b = 0; b < np && rc == POLAR_OK; ++b) {
+      if (!queued[b]) continue;
+      const cudaError_t q = cudaEventQuery(ev[b]);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) {
+        rc = set_cuda_error("batch poll", q);
+        break;
+      }
+      progressed = true;
+      queued[b] = 0;
+      rc = S[b].check();
+      if (rc != POLAR_OK) break;
+      if (S[b].done) {
+        --live;
+        continue;
+      }
+      rc = S[b].launch();
+      if (rc == POLAR_OK && cudaEventRecord(ev[b], ss[b]) != cudaSuccess) rc = set_cuda_error("batch event", cudaGetLastError());
+      queued[b] = 1;
+    }
+    if (!progressed) std::this_thread::yield();
+  }
+  // the caller's stream waits for every problem's stream
+  for (int b = 0; b < np; ++b)
+    if (ss[b]) {
+      if (cudaEventRecord(ev[b], ss[b]) == cudaSuccess) cudaStreamWaitEvent(st, ev[b], 0);
+    }
+  if (timing_on()) timing_collect();
+  out.assign(np, MkResult{});
+  for (int b = 0; b < np; ++b) {
+    if (rc == POLAR_OK) cudaStreamSynchronize(ss[b]);
+    out[b] = S[b].res;
+    S[b].cleanup();
+    if (ev[b]) cudaEventDestroy(ev[b]);
+    if (ss[b]) cudaStreamDestroy(ss[b]);
+  }
+  if (ready) cudaEventDestroy(ready);
+  return rc;
 }
 
 }  // namespace polar
@@ -919,6 +1052,8 @@ namespace polar {
 
 #define POLAR_MK_INST(T, VEC, W, E)                                                                 \
   template int mk_solve<T, VEC, W, E>(const SolvePrm<T>&, SolvePrm<T>*, cudaStream_t, MkResult*); \
+  template int mk_solve_batch<T, VEC, W, E>(const std::vector<SolvePrm<T>>&, const std::vector<double>&, \
+                                            cudaStream_t, std::vector<MkResult>&);                   \
   template int mk_grid_max<T, VEC, W, E>();
 
 POLAR_MK_INST(float, 4, false, POLAR_E32)

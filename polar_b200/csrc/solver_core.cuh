@@ -35,8 +35,15 @@ template <typename T> struct SolvePrm {
   int x_f32, ldx;
   double* h_out;
   long long* iters_out;
-  // workspace
-  T *r, *d, *v, *hist, *Pb, *Xb;
+  // workspace.  The residual r and the direction recurrence are FP64 in every precision:
+  // rounding either to FP32 every iteration breaks the local orthogonality and conjugacy
+  // of the CG recurrence enough to cost ~25 % more iterations on badly conditioned
+  // Laplacians.  d is the SpMM's gathered input in T; with T = float, dd holds the FP64
+  // direction and d its rounded copy (dd == nullptr: d is the direction itself).  v, the
+  // history and the shifted iterates are T.
+  double* r;
+  double* dd;
+  T *d, *v, *hist, *Pb, *Xb;
   typename AccOf<T>::type* chunk_part;
   int* hcount;
   double* part;
@@ -52,6 +59,29 @@ template <typename T> struct SolvePrm {
   long long* stats;  // [0]=iterations [1]=flushes [2..7]=phase ns (CTA 0 view)
   uint64_t timeout_ns;
 };
+
+// Direction d of one row item in FP64: from dd when the FP64 recurrence is kept apart from
+// the SpMM's copy, else from d.  store_dir writes both.
+template <typename T, int VEC>
+POLAR_D void load_dir(const SolvePrm<T>& P, double (&out)[VEC], size_t o) {
+  if (P.dd) {
+    vload<double, VEC>(out, P.dd + o);
+  } else {
+    T t[VEC];
+    vload<T, VEC>(t, P.d + o);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) out[v] = (double)t[v];
+  }
+}
+
+template <typename T, int VEC>
+POLAR_D void store_dir(const SolvePrm<T>& P, const double (&in)[VEC], size_t o) {
+  if (P.dd) vstore<double, VEC>(P.dd + o, in);
+  T t[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) t[v] = (T)in[v];
+  vstore<T, VEC>(P.d + o, t);
+}
 
 // ---------------------------------------------------------------------------------------
 template <int VEC>

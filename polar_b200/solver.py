@@ -43,6 +43,21 @@ def max_columns(prec):
 
 
 _WS = {}
+def tuned_layouts(G):
+    """The graph's SpMM layouts recorded by autotune.tune_msolve, keyed by (precision,
+    padded width): (lane bytes, sliced-ELL on/off, heavy-row threshold)."""
+    d = getattr(G, "_spmm_tuned", None)
+    if d is None:
+        d = {}
+        G._spmm_tuned = d
+    return d
+
+
+def _padded(prec, R):
+    ld = 1
+    while ld < R:
+        ld *= 2
+    return max(ld, 4 if prec == _lib.POLAR_MIXED else 2)
 
 
 def workspace(nbytes, device):
@@ -116,15 +131,25 @@ def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, *, 
     for lo in range(0, R, maxc):
         hi = min(R, lo + maxc)
         r = hi - lo
-        g = op.struct(heavy_thresh=lib.polar_heavy_threshold(prec, r), sell_rows=lib.polar_sell_rows(prec, r))
-        need = lib.polar_msolve_workspace_bytes(g, prec, r, p, nA)
-        ws = workspace(need, dev)
-        hpart = torch.zeros((p, r), dtype=torch.float64, device=dev) if track else None
-        xo = out[:, :, out_col + lo:]
-        st = lib.polar_msolve(g, prec, W[:, lo:].data_ptr(), ldw, r, tau_d.data_ptr(), p, act_d.data_ptr(),
-                              pos_d.data_ptr(), nA, float(tol), int(maxit), 1 if track else 0, xo.data_ptr(), x_f32,
-                              out.shape[2], hpart.data_ptr() if track else None, iters[lo:].data_ptr(),
-                              ws.data_ptr(), ws.numel(), stream)
+        cfg = tuned_layouts(G).get((int(prec), _padded(prec, r)))
+        if cfg is not None:
+            lib.polar_set_spmm_lane_bytes(cfg[0])
+            lib.polar_set_sell(cfg[1])
+        try:
+            thresh = cfg[2] if cfg is not None else lib.polar_heavy_threshold(prec, r)
+            g = op.struct(heavy_thresh=thresh, sell_rows=lib.polar_sell_rows(prec, r))
+            need = lib.polar_msolve_workspace_bytes(g, prec, r, p, nA)
+            ws = workspace(need, dev)
+            hpart = torch.zeros((p, r), dtype=torch.float64, device=dev) if track else None
+            xo = out[:, :, out_col + lo:]
+            st = lib.polar_msolve(g, prec, W[:, lo:].data_ptr(), ldw, r, tau_d.data_ptr(), p, act_d.data_ptr(),
+                                  pos_d.data_ptr(), nA, float(tol), int(maxit), 1 if track else 0, xo.data_ptr(),
+                                  x_f32, out.shape[2], hpart.data_ptr() if track else None, iters[lo:].data_ptr(),
+                                  ws.data_ptr(), ws.numel(), stream)
+        finally:
+            if cfg is not None:  # back to the automatic layout
+                lib.polar_set_spmm_lane_bytes(0)
+                lib.polar_set_sell(1)
         _lib.check(st, "polar_msolve")
         inf = _lib.MsolveInfo()
         st = lib.polar_msolve_finish(ws.data_ptr(), stream, inf)

@@ -6,7 +6,7 @@ for them. Host-side NumPy: this is input generation, not part of the timed path.
 """
 import numpy as np
 
-__all__ = ["chung_lu", "candidates", "CONFIGS", "make_config"]
+__all__ = ["chung_lu", "candidates", "CONFIGS", "make_config", "batch_specs"]
 
 
 def _chung_lu_weights(n, mean_deg, gamma, dmax):
@@ -122,7 +122,24 @@ CONFIGS = {
                         N=4096, K=24, q=64, B=16, k=0, sigma=1e-2, s=0.5, tol=1e-7),
     "full-n4M": dict(n=3997962, mean_deg=2 * 34681189 / 3997962, gamma=2.1, seed=4, dmax=15000, min_degree=1,
                      N=1000000, K=32, q=64, B=16, k=100, sigma=1e-2, s=0.5, tol=1e-6),
+    # many graphs solved together: per-graph shapes from batch_specs; each graph's bank
+    # solve (2q right-hand sides) over the endpoints of up to N candidates
+    "batch48": dict(graphs=48, N=20000, K=16, q=32, k=10, tol=1e-7),
 }
+
+
+def batch_specs(count=48, seed=3):
+    """Per-graph shapes of the many-graphs workload: n log-uniform in [5k, 400k], mean
+    degree uniform in [4, 20], exponent uniform in [2.2, 2.8], sigma from {1e-3, 1e-2,
+    1e-1} and s from {0.3, 0.5, 0.7}, each drawn per graph from one seeded stream."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for g in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(5e3), np.log(4e5)))))
+        out.append(dict(n=n, mean_deg=float(rng.uniform(4.0, 20.0)), gamma=float(rng.uniform(2.2, 2.8)),
+                        seed=1000 + g, sigma=float(rng.choice([1e-3, 1e-2, 1e-1])),
+                        s=float(rng.choice([0.3, 0.5, 0.7]))))
+    return out
 
 
 def make_config(name, n=None, N=None, cand_seed=None):

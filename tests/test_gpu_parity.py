@@ -100,7 +100,8 @@ def test_msolve_fp64_matches_reference(gold, torch_cuda):
 def test_msolve_persistent_driver(gold, torch_cuda, prec):
     """The single-launch cooperative driver gives the same solves as the graph driver.  In
     mixed precision the graph driver sums each SpMM row in FP64 and the persistent driver in
-    FP32, so the graph driver needs no more iterations and the solves agree to 1e-5."""
+    FP32, so the graph driver needs no more iterations, and the two agree within the mixed
+    solver's bounds against the reference (1e-4 for the iterates, 1e-5 for the norms)."""
     import polar_b200 as pg
     from polar_b200.solver import set_solver_mode
     z, op = _ms_inputs(gold, pg)
@@ -115,9 +116,9 @@ def test_msolve_persistent_driver(gold, torch_cuda, prec):
         assert np.max(np.abs(itg - itp)) <= 3  # different reduction order
     else:
         assert np.all(itg <= itp + 3)
-    lim = 1e-8 if prec == "fp64" else 1e-5
+    lim, hlim = (1e-8, 1e-8) if prec == "fp64" else (1e-4, 1e-5)
     assert _rel(Xp.cpu().numpy(), Xg.cpu().numpy()) < lim
-    assert _rel(hp.cpu().numpy(), hg.cpu().numpy()) < lim
+    assert _rel(hp.cpu().numpy(), hg.cpu().numpy()) < hlim
 
 
 def test_msolve_mixed_close_to_reference(gold, torch_cuda):

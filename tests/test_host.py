@@ -134,3 +134,24 @@ def test_status_mapping():
         _lib.check(_lib.POLAR_ERR_ITER_CAP)
     with pytest.raises(_lib.PolarError):
         _lib.check(_lib.POLAR_ERR_BAD_ARG, "x")
+
+
+def test_batch_problem_struct_matches_header(tmp_path):
+    """ctypes' polar_msolve_problem has the C layout: size and every field offset, as gcc
+    lays out the struct declared in include/polar.h."""
+    import ctypes
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    names = [f[0] for f in _lib.MsolveProblem._fields_]
+    src = tmp_path / "layout.c"
+    body = "".join(f'  printf("{nm} %zu\\n", offsetof(polar_msolve_problem, {nm}));\n' for nm in names)
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "polar.h"\nint main(void) {\n'
+                   '  printf("size %zu\\n", sizeof(polar_msolve_problem));\n' + body + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)])
+    got = dict(line.split() for line in subprocess.check_output([str(exe)], text=True).splitlines())
+    assert int(got["size"]) == ctypes.sizeof(_lib.MsolveProblem)
+    for nm in names:
+        assert int(got[nm]) == getattr(_lib.MsolveProblem, nm).offset, nm
