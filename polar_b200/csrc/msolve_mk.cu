@@ -155,6 +155,9 @@ POLAR_D void apply_added_edges(const SolvePrm<T>& P, double* tmp, double* s_col)
 #ifndef POLAR_RESID_U
 #define POLAR_RESID_U 2   // same for the r update (more spills at 64 registers)
 #endif
+#ifndef POLAR_STREAM_MINB
+#define POLAR_STREAM_MINB 2  // resident 512-thread CTAs per SM requested for the r and d updates
+#endif
 // SpMM accumulator: FP64 row sums for FP32 vectors unless POLAR_SPMM_ACC64 = 0.  A
 // Laplacian row (deg + sigma + shift) x_i - sum_j x_j cancels heavily for smooth vectors, so
 // the neighbour sum is kept unrounded until that final combination (one rounding per row
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
 
 // ---- r <- r - a v, history, r.r, column scalars -----------------------------------------
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ SolvePrm<T> P, int slot) {
+__global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_resid(const __grid_constant__ SolvePrm<T> P, int slot) {
 
   pdl_wait();
   pdl_launch();
@@ -513,7 +516,7 @@ __global__ void __launch_bounds__(kBlock, 2) mk_resid(const __grid_constant__ So
 
 // ---- pole recurrences + d <- r + beta d -------------------------------------------------
 template <typename T, int VEC>
-__global__ void __launch_bounds__(kBlock, 2) mk_dir(const __grid_constant__ SolvePrm<T> P, int slot) {
+__global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_dir(const __grid_constant__ SolvePrm<T> P, int slot) {
 
   pdl_wait();
   pdl_launch();

@@ -155,3 +155,56 @@ def test_batch_problem_struct_matches_header(tmp_path):
     assert int(got["size"]) == ctypes.sizeof(_lib.MsolveProblem)
     for nm in names:
         assert int(got[nm]) == getattr(_lib.MsolveProblem, nm).offset, nm
+
+
+def test_autotune_lane_resolution_matches_library():
+    """The tuner's model of how lane bytes resolve to lanes per row agrees with the
+    library's sliced-ELL height (32 / lanes) for every width and precision (host-only
+    calls, no device needed)."""
+    from polar_b200 import autotune
+    lib = _lib.load()
+    try:
+        for prec in (_lib.POLAR_FP64, _lib.POLAR_MIXED):
+            maxc = 128 if prec == _lib.POLAR_MIXED else 64
+            for R in (1, 3, 8, 16, 33, 64, maxc):
+                if R > maxc:
+                    continue
+                ld = autotune._ld(prec, R)
+                for lb in (16, 32, 64):
+                    lib.polar_set_spmm_lane_bytes(lb)
+                    lanes = autotune._lanes(prec, ld, lb)
+                    assert lib.polar_sell_rows(prec, R) == 32 // lanes, (prec, R, lb)
+                    assert lib.polar_heavy_threshold(prec, R) == max(16, 8 * lanes), (prec, R, lb)
+    finally:
+        lib.polar_set_spmm_lane_bytes(0)
+
+
+def test_batch_rejects_bad_arguments_before_launch():
+    """polar_msolve_batch checks its arguments on the host: no problems, too many, an
+    unknown precision and a missing pointer are BAD_ARG without touching a device."""
+    import ctypes
+    lib = _lib.load()
+    assert lib.polar_msolve_batch(None, 1, _lib.POLAR_FP64, None) == _lib.POLAR_ERR_BAD_ARG
+    probs = (_lib.MsolveProblem * 65)()
+    assert lib.polar_msolve_batch(probs, 0, _lib.POLAR_FP64, None) == _lib.POLAR_ERR_BAD_ARG
+    assert lib.polar_msolve_batch(probs, 65, _lib.POLAR_FP64, None) == _lib.POLAR_ERR_BAD_ARG
+    assert lib.polar_msolve_batch(probs, 1, 7, None) == _lib.POLAR_ERR_BAD_ARG
+    g = _lib.PolarGraph()
+    g.n = 10
+    probs[0].g = ctypes.pointer(g)
+    probs[0].R = 4
+    assert lib.polar_msolve_batch(probs, 1, _lib.POLAR_FP64, None) == _lib.POLAR_ERR_BAD_ARG
+    assert b"null pointer" in lib.polar_last_error()
+
+
+def test_batch_specs_follow_the_workload_rules():
+    """The 48-graph workload: n log-uniform in [5k, 400k], mean degree in [4, 20],
+    exponent in [2.2, 2.8], sigma and s from their three values; seeded."""
+    from polar_b200.synth import batch_specs
+    sp = batch_specs()
+    assert len(sp) == 48 and sp == batch_specs()
+    assert all(5000 <= x["n"] <= 400000 for x in sp)
+    assert all(4.0 <= x["mean_deg"] <= 20.0 and 2.2 <= x["gamma"] <= 2.8 for x in sp)
+    assert {x["sigma"] for x in sp} == {1e-3, 1e-2, 1e-1}
+    assert {x["s"] for x in sp} == {0.3, 0.5, 0.7}
+    assert len({x["seed"] for x in sp}) == 48
