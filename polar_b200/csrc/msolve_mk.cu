@@ -1036,7 +1036,9 @@ int mk_solve_batch(const std::vector<SolvePrm<T>>& Ps, const std::vector<double>
   if (timing_on()) timing_collect();
   out.assign(np, MkResult{});
   for (int b = 0; b < np; ++b) {
-    if (rc == POLAR_OK) cudaStreamSynchronize(ss[b]);
+    // drain every stream before its graph is destroyed (also after an error elsewhere)
+    if (ss[b] && cudaStreamSynchronize(ss[b]) != cudaSuccess && rc == POLAR_OK)
+      rc = set_cuda_error("batch drain", cudaGetLastError());
     out[b] = S[b].res;
     S[b].cleanup();
     if (ev[b]) cudaEventDestroy(ev[b]);
