@@ -215,6 +215,25 @@ typedef struct polar_msolve_problem {
 size_t polar_msolve_batch_workspace_bytes(const polar_graph* g, int precision, int R, int p, int nA);
 int polar_msolve_batch(const polar_msolve_problem* probs, int nprob, int precision, polar_stream_t stream);
 
+/* ---- sketch construction (realworld/polar_gpu.py:137-165: _block_rows, sketches) ----
+ * polar_block_orth: d_G holds ceil(rows/q) Gaussian q x q blocks, row-major
+ * (G[b][r][j]), in the order the reference draws them.  Each block's columns are
+ * orthonormalised in order (QR with a positive diagonal of R, as the reference's
+ * sign-fixed numpy QR); row b*q + i of W (rows x q, ldw) receives column i of block b's
+ * Q, times d_scale[b*q + i] when d_scale is given (the reference's U *= sqrt(w)).  q <= 128.
+ * polar_center_columns: W (rows x q) -= its column means (the reference's W - W.mean(0)),
+ * with a caller scratch of polar_center_columns_tmp_bytes(q).
+ * polar_incidence_apply: F[i] += sum_k sign[k] * U[eidx[k]] over the CSR row i
+ * (indptr n+1, eidx and int8 sign per entry): F += C^T U for one edge chunk of the
+ * reference's F = C_0^T U. */
+int polar_block_orth(const double* d_G, int64_t rows, int q, const double* d_scale, double* d_W, int ldw,
+                     polar_stream_t stream);
+size_t polar_center_columns_tmp_bytes(int q);
+int polar_center_columns(double* d_W, int64_t rows, int q, int ldw, void* d_tmp, size_t tmp_bytes,
+                         polar_stream_t stream);
+int polar_incidence_apply(int n, const int32_t* d_indptr, const int32_t* d_eidx, const int8_t* d_sign,
+                          const double* d_U, int ldu, int q, double* d_F, int ldf, polar_stream_t stream);
+
 /* ---- incidence right-hand sides (polar_gpu.py:225-226, 282) ----
  * For c < R with e = sel[c] and (a, b) = cand[e] (cand: int64 [N][2]):
  * W[:, c] = e_a - e_b (n x R FP64, ldw; zeroed first).  When d_es (int32 [N][2], the

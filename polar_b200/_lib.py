@@ -100,6 +100,10 @@ SIGNATURES = {
     "polar_set_sell": (None, [_I]),
     "polar_msolve_batch_workspace_bytes": (_S, [_GP, _I, _I, _I, _I]),
     "polar_msolve_batch": (_I, [ctypes.POINTER(MsolveProblem), _I, _I, _P]),
+    "polar_block_orth": (_I, [_P, _I64, _I, _P, _P, _I, _P]),
+    "polar_center_columns_tmp_bytes": (_S, [_I]),
+    "polar_center_columns": (_I, [_P, _I64, _I, _I, _P, _S, _P]),
+    "polar_incidence_apply": (_I, [_I, _P, _P, _P, _P, _I, _I, _P, _I, _P]),
     "polar_fill_incidence": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _P, _P]),
     "polar_pair_norms": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _I, _P, _P]),
     "polar_topb_tmp_bytes": (_S, [_I, _I]),

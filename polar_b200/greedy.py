@@ -52,6 +52,14 @@ class _Phase:
         return out
 
 
+def _f64_on(x, dev):
+    """A sketch array (host NumPy, or a device tensor from sketches(..., device=True)) as
+    a float64 tensor on `dev`."""
+    if isinstance(x, torch.Tensor):
+        return x.to(device=dev, dtype=torch.float64)
+    return torch.as_tensor(np.ascontiguousarray(x, dtype=np.float64)).to(dev)
+
+
 def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=None, naive=False, seed=2026,
           kind="block", trace=None, time_limit=None, *, K=None, precision="fp64", width=None, maxit=100000,
           phases=False):
@@ -72,7 +80,7 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
     if sketch is None:
         sketch = sketches(G, cand, q, seed, kind)
     Z, F, Gc = sketch
-    q = int(np.shape(Z)[1])
+    q = int(Z.shape[1])
     lib = _lib.load()
     stream = torch.cuda.current_stream(dev).cuda_stream
 
@@ -88,9 +96,9 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
     ea_d = es_d[:, 0].contiguous()
     eb_d = es_d[:, 1].contiguous()
     RHS = torch.empty((n, 2 * q), dtype=torch.float64, device=dev)
-    RHS[:, :q] = torch.as_tensor(np.asarray(Z, dtype=np.float64)).to(dev)
-    RHS[:, q:] = torch.as_tensor(np.asarray(F, dtype=np.float64)).to(dev)
-    Gd = torch.as_tensor(np.ascontiguousarray(Gc, dtype=np.float64)).to(dev)
+    RHS[:, :q] = _f64_on(Z, dev)
+    RHS[:, q:] = _f64_on(F, dev)
+    Gd = _f64_on(Gc, dev).contiguous()
     live_d = torch.ones(N, dtype=torch.uint8, device=dev)
     XY = torch.empty((p, nA, 2 * q), dtype=xdt, device=dev)
     h = torch.empty((p, N), dtype=torch.float64, device=dev)
