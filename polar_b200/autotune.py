@@ -31,10 +31,7 @@ HEAVY_MULT = (4, 8, 16, 32)
 
 
 def _ld(prec, R):
-    ld = 1
-    while ld < R:
-        ld *= 2
-    return max(ld, 4 if prec == _lib.POLAR_MIXED else 2)
+    return _solver._padded(prec, R)
 
 
 def tuned(G, precision, R):

@@ -43,6 +43,8 @@ def max_columns(prec):
 
 
 _WS = {}
+
+
 def tuned_layouts(G):
     """The graph's SpMM layouts recorded by autotune.tune_msolve, keyed by (precision,
     padded width): (lane bytes, sliced-ELL on/off, heavy-row threshold)."""
@@ -54,6 +56,7 @@ def tuned_layouts(G):
 
 
 def _padded(prec, R):
+    """The solver's padded width for R columns: next power of two, at least one vector."""
     ld = 1
     while ld < R:
         ld *= 2
