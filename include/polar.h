@@ -120,8 +120,8 @@ int polar_version(void);
  * 2 direction/pole update, 3 deferred update, 4 init, the number of timed launches, their
  * summed device time (ms) and summed algorithmic bytes (SpMM, both launches together,
  * counted on class 0: 4(n+1) + 4 nnz + 2 s n R; residual, r in FP64: (16 + s) n R + s nA R;
- * direction: 24 n R in FP64, 28 n R in mixed precision (FP64 r and direction in, FP64
- * direction and its FP32 copy out); deferred update: (4p + M) s nA R). */
+ * direction: 24 n R (r and the direction in, the direction out; in mixed precision the
+ * direction is an FP32 value plus its FP32 remainder); deferred update: (4p + M) s nA R). */
 long long polar_launch_count(void);
 void polar_set_kernel_timing(int on);
 int polar_kernel_timing(int cls, long long* launches, double* ms, double* bytes);

@@ -68,17 +68,14 @@ POLAR_D void msolve_run(const SolvePrm<T>& P, const int vb, const int vnb) {
     for (long long e = tid; e < nvec; e += nth) {
       const long long i = e / rg.G;
       double wd[VEC];
-      T w[VEC];
 #pragma unroll
       for (int v = 0; v < VEC; ++v) {
         const int c = rg.col + v;
         wd[v] = (c < P.R) ? __ldg(P.W + (size_t)i * P.ldw + c) : 0.0;
-        w[v] = (T)wd[v];
         acc[v] += wd[v] * wd[v];
       }
       vstore<double, VEC>(P.r + (size_t)i * ld + rg.col, wd);
-      if (P.dd) vstore<double, VEC>(P.dd + (size_t)i * ld + rg.col, wd);
-      vstore<T, VEC>(P.d + (size_t)i * ld + rg.col, w);
+      store_dir<T, VEC>(P, wd, (size_t)i * ld + rg.col);
     }
     reduce_cols_to_part<VEC>(acc, rg.G, ld, red, my_part);
   }
@@ -438,7 +435,7 @@ static void solve_layout(const polar_graph* g, int precision, int R, int p, int 
   add(4096);                                       // 30 device copy of the parameter block
   add((size_t)p * ld * kNC * 8);                   // 31 composed deferred-update coefficients
   add((size_t)kMaxHeavyCtas * ld * 8);             // 32 heavy-row d.v partials
-  add(precision == POLAR_MIXED ? n * ld * 8 : 0);  // 33 FP64 direction (mixed precision)
+  add(precision == POLAR_MIXED ? n * ld * 4 : 0);  // 33 direction remainder (mixed precision)
   L->total = o;
   L->ld = ld;
   L->vec = choose_vec(precision, ld);
@@ -590,7 +587,7 @@ static void fill_prm(SolvePrm<TT>& prm, const polar_graph* g, int R, int ld, int
   prm.chig = (double*)(ws + L.off[29]);
   prm.cmp = composed ? (double*)(ws + L.off[31]) : nullptr;
   prm.part_h = (double*)(ws + L.off[32]);
-  prm.dd = sizeof(TT) == 4 ? (double*)(ws + L.off[33]) : nullptr;
+  prm.dlo = sizeof(TT) == 4 ? (float*)(ws + L.off[33]) : nullptr;
   prm.nbh = 0;
   prm.timeout_ns = g_timeout_ns;
 }

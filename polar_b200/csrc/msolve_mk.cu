@@ -76,17 +76,14 @@ __global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolveP
   for (long long e = tid; e < nvec; e += nth) {
     const long long i = e >> lgG;
     double wd[VEC];
-    T w[VEC];
 #pragma unroll
     for (int v = 0; v < VEC; ++v) {
       const int c = rg.col + v;
       wd[v] = (c < P.R) ? __ldg(P.W + (size_t)i * P.ldw + c) : 0.0;
-      w[v] = (T)wd[v];
       acc[v] += wd[v] * wd[v];
     }
     vstore<double, VEC>(P.r + (size_t)i * ld + rg.col, wd);
-    if (P.dd) vstore<double, VEC>(P.dd + (size_t)i * ld + rg.col, wd);
-    vstore<T, VEC>(P.d + (size_t)i * ld + rg.col, w);
+    store_dir<T, VEC>(P, wd, (size_t)i * ld + rg.col);
   }
   reduce_cols_to_part<VEC>(acc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
   if (last_cta(P.ctl + C_CNT0)) {
@@ -841,9 +838,9 @@ struct MkSolver {
     const double s = sizeof(T), n = P.n, R = P.R, nA = P.nA;
     // algorithmic bytes per launch (unweighted CSR: values implicit, diagonal from indptr)
     const double b_spmm = 4.0 * (n + 1) + 4.0 * P.g.nnz + 2.0 * s * n * R;
-    // r is FP64 in both precisions; mixed precision keeps an FP64 direction beside d
+    // r is FP64 in both precisions; mixed precision keeps the direction's FP32 remainder
     const double b_resid = (16.0 + s) * n * R + s * nA * R;
-    const double b_dir = (s == 4.0 ? 28.0 : 24.0) * n * R;  // mixed: r, dd in; dd, d out
+    const double b_dir = 24.0 * n * R;  // r (8) + direction (8) in, direction (8) out
     b_flush = (4.0 * P.p + kHist) * s * nA * R;
     const int g0 = scaled(occ_grid(mk_init<T, VEC>, kBlock), f, 1);
     const int cpl = spmm_cpl<T>(P.ld, VEC);

@@ -35,14 +35,16 @@ template <typename T> struct SolvePrm {
   int x_f32, ldx;
   double* h_out;
   long long* iters_out;
-  // workspace.  The residual r and the direction recurrence are FP64 in every precision:
-  // rounding either to FP32 every iteration breaks the local orthogonality and conjugacy
-  // of the CG recurrence enough to cost ~25 % more iterations on badly conditioned
-  // Laplacians.  d is the SpMM's gathered input in T; with T = float, dd holds the FP64
-  // direction and d its rounded copy (dd == nullptr: d is the direction itself).  v, the
-  // history and the shifted iterates are T.
+  // workspace.  The residual r and the direction recurrence are kept to FP64 accuracy in
+  // every precision: rounding either to FP32 every iteration breaks the local
+  // orthogonality and conjugacy of the CG recurrence enough to cost ~25 % more iterations
+  // on badly conditioned Laplacians.  d is the SpMM's gathered input in T.  With
+  // T = float the direction is the pair d + dlo (dlo = the FP32 remainder of the FP64
+  // value, 48 significant bits together), so the SpMM reads d alone and the recurrence
+  // reads both; dlo == nullptr: d is the direction itself.  v, the history and the
+  // shifted iterates are T.
   double* r;
-  double* dd;
+  float* dlo;
   T *d, *v, *hist, *Pb, *Xb;
   typename AccOf<T>::type* chunk_part;
   int* hcount;
@@ -60,27 +62,34 @@ template <typename T> struct SolvePrm {
   uint64_t timeout_ns;
 };
 
-// Direction d of one row item in FP64: from dd when the FP64 recurrence is kept apart from
-// the SpMM's copy, else from d.  store_dir writes both.
+// Direction of one row item in FP64: d (+ dlo when the remainder is kept).  store_dir
+// writes d = (T)x and, with a remainder, dlo = (float)(x - d).
 template <typename T, int VEC>
 POLAR_D void load_dir(const SolvePrm<T>& P, double (&out)[VEC], size_t o) {
-  if (P.dd) {
-    vload<double, VEC>(out, P.dd + o);
-  } else {
-    T t[VEC];
-    vload<T, VEC>(t, P.d + o);
+  T hi[VEC];
+  vload<T, VEC>(hi, P.d + o);
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) out[v] = (double)t[v];
+  for (int v = 0; v < VEC; ++v) out[v] = (double)hi[v];
+  if (P.dlo) {
+    float lo[VEC];
+    vload<float, VEC>(lo, P.dlo + o);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) out[v] += (double)lo[v];
   }
 }
 
 template <typename T, int VEC>
 POLAR_D void store_dir(const SolvePrm<T>& P, const double (&in)[VEC], size_t o) {
-  if (P.dd) vstore<double, VEC>(P.dd + o, in);
-  T t[VEC];
+  T hi[VEC];
 #pragma unroll
-  for (int v = 0; v < VEC; ++v) t[v] = (T)in[v];
-  vstore<T, VEC>(P.d + o, t);
+  for (int v = 0; v < VEC; ++v) hi[v] = (T)in[v];
+  vstore<T, VEC>(P.d + o, hi);
+  if (P.dlo) {
+    float lo[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) lo[v] = (float)(in[v] - (double)hi[v]);
+    vstore<float, VEC>(P.dlo + o, lo);
+  }
 }
 
 // ---------------------------------------------------------------------------------------
