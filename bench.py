@@ -333,6 +333,9 @@ def run_ours(a):
             "parity": parity,
             "sequence_head": mixed["sequence"][:8],
             "spmv": mixed["spmv"], "p": mixed["p"],
+            "cg": {"seed_iterations": int(sum(it for _, it in mixed["solves"])), "column_iterations": mixed["spmv"],
+                   "seed_iterations_per_s": sum(it for _, it in mixed["solves"]) / per,
+                   "column_iterations_per_s": mixed["spmv"] / per},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "autotune": tuned or None,
