@@ -218,7 +218,7 @@ def run_ours(a):
     if not a.no_autotune:
         # SpMM layout per solve width (shortlist B, bank 2q), timed once before any greedy
         from polar_b200 import autotune
-        for prec, wide in (("mixed", 128), ("fp64", 64)):
+        for prec, wide in (("mixed", 128),) + ((("fp64", 64),) if not a.no_fp64 else ()):
             for R in sorted({c["B"], min(2 * c["q"], wide)}):
                 t = autotune.tune_msolve(pg.Op(G), R, prec, p=c["K"])
                 tuned[f"{prec}_R{R}"] = {"lane_bytes": t["best"][0], "sliced_ell": t["best"][1],
