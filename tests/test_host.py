@@ -208,3 +208,46 @@ def test_batch_specs_follow_the_workload_rules():
     assert {x["sigma"] for x in sp} == {1e-3, 1e-2, 1e-1}
     assert {x["s"] for x in sp} == {0.3, 0.5, 0.7}
     assert len({x["seed"] for x in sp}) == 48
+
+
+def test_batch_cta_split(tmp_path):
+    """The persistent batch driver's CTA split (csrc/batch_split.h, host C++): every
+    problem gets at least one CTA and at most its cap, the total never exceeds the grid,
+    spare CTAs go out in proportion to cost, and a grid larger than the caps allow is
+    left partly unused."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    src = tmp_path / "split.cc"
+    src.write_text(r'''
+#include <cstdio>
+#include "batch_split.h"
+int main() {
+  using polar::split_ctas;
+  std::vector<int> c;
+  split_ctas({1, 1, 1, 1}, {100, 100, 100, 100}, 8, c);
+  printf("%d %d %d %d\n", c[0], c[1], c[2], c[3]);
+  split_ctas({1, 3}, {100, 100}, 10, c);
+  printf("%d %d\n", c[0], c[1]);
+  split_ctas({1, 1000}, {100, 3}, 50, c);
+  printf("%d %d\n", c[0], c[1]);
+  split_ctas({5, 1, 1}, {2, 2, 2}, 148, c);
+  printf("%d %d %d\n", c[0], c[1], c[2]);
+  split_ctas({1, 2, 3, 4, 5}, {1000, 1000, 1000, 1000, 1000}, 148, c);
+  int s = 0;
+  for (int x : c) s += x;
+  printf("%d %d %d %d %d %d\n", c[0], c[1], c[2], c[3], c[4], s);
+  return 0;
+}
+''')
+    exe = tmp_path / "split"
+    subprocess.check_call(["g++", "-std=c++17", "-I", str(ROOT / "polar_b200" / "csrc"), str(src), "-o", str(exe)])
+    out = [list(map(int, ln.split())) for ln in subprocess.check_output([str(exe)], text=True).splitlines()]
+    assert out[0] == [2, 2, 2, 2]                 # equal costs share evenly
+    assert out[1] == [3, 7]                       # 8 spare CTAs split 1:3 (2 and 6), one more by remainder
+    assert out[2] == [47, 3]                      # the costly problem is capped, the rest goes on
+    assert out[3] == [2, 2, 2]                    # caps bound the total below the grid
+    c = out[4]
+    assert c[5] == 148 and all(x >= 1 for x in c[:5])
+    assert c[:5] == sorted(c[:5])                 # more cost, no fewer CTAs
