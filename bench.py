@@ -330,6 +330,7 @@ def run_ours(a):
                          "measured": "CUDA events around every solver kernel in one instrumented greedy run "
                                      "right after the timed region (%.3f s with events)" % inst["device_s"]},
             "kernels": kernels,
+            "iteration_alg_GBps": (sum(v[2] for v in ktime.values()) / (ktot / 1e3) / 1e9) if ktot else None,
             "parity": parity,
             "sequence_head": mixed["sequence"][:8],
             "spmv": mixed["spmv"], "p": mixed["p"],
