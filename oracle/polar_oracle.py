@@ -15,7 +15,7 @@ import time
 import numpy as np
 import scipy.sparse as sp
 
-__all__ = ["composite", "fixed_rule", "poles", "Graph", "Op", "msolve", "sketches",
+__all__ = ["composite", "fixed_rule", "poles", "Graph", "Op", "msolve", "sketches", "candidates",
            "polar", "true_marginals", "degree_greedy", "random_set", "chunk_width"]
 
 
@@ -148,7 +148,7 @@ class Counter:
         self.rhs = 0
 
 
-def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None):
+def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, on_iteration=None):
     """Multi-shift CG for (M + tau_j I) U = W over all poles and columns
     (polar_gpu.py:88-133).
 
@@ -212,6 +212,8 @@ def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None):
         ap = np.where(act, a, ap)
         bp = np.where(act, be, bp)
         act &= ~done
+        if on_iteration is not None:
+            on_iteration(it)  # the benchmark's CPU baseline times single iterations
         if it % 8 == 7 and not act.any():
             break
     else:
@@ -286,7 +288,6 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
     active = np.unique(cand)
     es = np.searchsorted(active, cand)
     ea, eb = es[:, 0], es[:, 1]
-    tcol = tau[:, None]
     ocol = om[:, None]
     op = Op(G)
     cnt = Counter()
@@ -306,9 +307,7 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
         return X, Y, h, t
 
     def proxy(h, t):
-        if obj == "logdet":
-            return np.log1p(t[0] + sigma * h[0])
-        return np.sum(ocol * h / (1.0 + t + (sigma + tcol) * h), axis=0)
+        return proxy_scores(h, t, om, tau, sigma, obj)
 
     X, Y, h, t = bank()
     for rnd in range(k):
@@ -345,21 +344,50 @@ def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=Non
         aa, bb = es[e]
         a, b = cand[e]
         if not naive and rnd + 1 < k:
-            xi = X[:, aa] - X[:, bb]
-            eta = Gc[e][None] - (Y[:, aa] - Y[:, bb])
-            D = 1.0 + u[:, aa] - u[:, bb]
-            cc = (u[:, ea] - u[:, eb]) / D[:, None]
-            wX = np.einsum("pnq,pq->pn", X, xi)
-            wY = np.einsum("pnq,pq->pn", Y, eta)
-            h = np.maximum(0.0, h - 2 * cc * (wX[:, ea] - wX[:, eb]) + cc * cc * np.sum(xi * xi, 1)[:, None])
-            t = np.maximum(0.0, t + 2 * cc * (wY[:, ea] - wY[:, eb]) + cc * cc * np.sum(eta * eta, 1)[:, None])
-            X -= u[:, :, None] * xi[:, None, :] / D[:, None, None]
-            Y += u[:, :, None] * eta[:, None, :] / D[:, None, None]
+            h, t = maintain(X, Y, h, t, u, Gc[e], aa, bb, ea, eb)
         F[a] += Gc[e]
         F[b] -= Gc[e]
         op.add(a, b)
     return dict(sequence=seq, marginals=marg, seconds=time.perf_counter() - t0, spmv=cnt.spmv,
                 rhs=cnt.rhs, p=p, rounds=len(seq), truncated=len(seq) < k)
+
+
+def proxy_scores(h, t, om, tau, sigma, obj="frac"):
+    """Proxy G^_e of every candidate from the caches (polar_gpu.py:208-211)."""
+    if obj == "logdet":
+        return np.log1p(t[0] + sigma * h[0])
+    return np.sum(om[:, None] * h / (1.0 + t + (sigma + tau[:, None]) * h), axis=0)
+
+
+def maintain(X, Y, h, t, u, g_e, aa, bb, ea, eb):
+    """Sherman–Morrison maintenance after the winner e = (aa, bb) joins the graph
+    (polar_gpu.py:242-249): X, Y updated in place; returns the new caches (h, t)."""
+    xi = X[:, aa] - X[:, bb]
+    eta = g_e[None] - (Y[:, aa] - Y[:, bb])
+    D = 1.0 + u[:, aa] - u[:, bb]
+    cc = (u[:, ea] - u[:, eb]) / D[:, None]
+    wX = np.einsum("pnq,pq->pn", X, xi)
+    wY = np.einsum("pnq,pq->pn", Y, eta)
+    h = np.maximum(0.0, h - 2 * cc * (wX[:, ea] - wX[:, eb]) + cc * cc * np.sum(xi * xi, 1)[:, None])
+    t = np.maximum(0.0, t + 2 * cc * (wY[:, ea] - wY[:, eb]) + cc * cc * np.sum(eta * eta, 1)[:, None])
+    X -= u[:, :, None] * xi[:, None, :] / D[:, None, None]
+    Y += u[:, :, None] * eta[:, None, :] / D[:, None, None]
+    return h, t
+
+
+def candidates(n, edges, N, seed):
+    """Uniform non-edge pool, one pair per draw (realworld/graphs.py:61-69): the rule the
+    batched polar_b200.synth.candidates must reproduce."""
+    keys = np.sort(np.asarray(edges, np.int64)[:, 0] * n + np.asarray(edges, np.int64)[:, 1])
+    rng = np.random.default_rng(seed)
+    chosen = set()
+    while len(chosen) < N:
+        u, v = sorted(map(int, rng.integers(n, size=2)))
+        i = np.searchsorted(keys, u * n + v)
+        if u != v and not (i < len(keys) and keys[i] == u * n + v):
+            chosen.add((u, v))
+    c = np.asarray(sorted(chosen), dtype=np.int64)
+    return np.ascontiguousarray(c[rng.permutation(N)])
 
 
 def degree_greedy(G, cand, k):
@@ -447,3 +475,116 @@ def relaxed_dense(n, edges, sigma, cand, w, s, tau=None, om=None):
         out["grad_q"] = np.array([sum(o * np.sum((d / (lw + t)) ** 2) for t, o in zip(tau, om)) for d in D])
         out["dsigma_q"] = float(-s * sum((o / t) * (phi(0.0) - phi(t)) for t, o in zip(tau, om)))
     return out
+
+
+# ---------------------------------------------------------------------------------------
+# Dense eigendecomposition oracles (realworld/exact.py), the small-graph certificate.
+def _dense_add(M, a, b):
+    M[a, a] += 1
+    M[b, b] += 1
+    M[a, b] -= 1
+    M[b, a] -= 1
+
+
+def frac_value(lam, s, obj):
+    """Objective of an eigenvalue set (exact.py:12-17)."""
+    if obj == "frac":
+        return float(np.sum(lam ** (-s)))
+    if obj == "er":
+        return float(np.sum(1.0 / lam))
+    return float(-np.sum(np.log(lam)))
+
+
+def twin_gain(M, pairs, s):
+    """Closed-form marginal for candidates joining non-adjacent twins (exact.py:20-28):
+    x^-s - (x + 2)^-s with x = M_uu; nan for other pairs."""
+    a = pairs[:, 0]
+    b = pairs[:, 1]
+    r = np.arange(len(pairs))
+    D = M[a] - M[b]
+    D[r, a] = 0
+    D[r, b] = 0
+    twin = (np.abs(D).max(1) == 0) & (M[a, b] == 0) & (M[a, a] == M[b, b])
+    x = M[a, a]
+    g = -x ** (-s) * np.expm1(-s * np.log1p(2 / x))
+    return np.where(twin, g, np.nan)
+
+
+def exact_greedy(M0, cand, k, s, obj="frac"):
+    """True-marginal greedy with eps = 1e-9 interval screening (exact.py:31-62)."""
+    M = np.array(M0, dtype=np.float64, copy=True)
+    live = np.ones(len(cand), bool)
+    seq, contenders = [], []
+    ea, eb = cand[:, 0], cand[:, 1]
+    for _ in range(k):
+        lam, V = np.linalg.eigh(M)
+        Wc = (V[ea] - V[eb]) ** 2
+        if obj == "er":
+            sc = (Wc @ lam ** -2) / (1 + Wc @ (1 / lam))
+            sc[~live] = -np.inf
+            e = int(np.argmax(sc))
+        elif obj == "logdet":
+            sc = np.log1p(Wc @ (1 / lam))
+            sc[~live] = -np.inf
+            e = int(np.argmax(sc))
+        else:
+            tau, om, eps = composite(s, float(lam[0]) * 0.999, float(lam[-1]) + 2.001, 1e-9)
+            eps = max(eps, 1e-9)
+            D = 1 / (lam[:, None] + tau[None])
+            sc = ((Wc @ (D * D)) / (1 + Wc @ D)) @ om
+            sc[~live] = -np.inf
+            best_lo = float(np.max(sc)) / (1 + eps)
+            ids = np.flatnonzero((sc / (1 - eps) >= best_lo) & live)
+            if len(ids) == 1:
+                e = int(ids[0])
+                contenders.append((1, 0))
+            else:
+                vals = np.empty(len(ids))
+                tw = twin_gain(M, cand[ids], s)
+                solved = 0
+                old = float(np.sum(lam ** -s))
+                for i, c in enumerate(ids):
+                    if np.isfinite(tw[i]):
+                        vals[i] = tw[i]
+                        continue
+                    A = M.copy()
+                    _dense_add(A, int(cand[c, 0]), int(cand[c, 1]))
+                    solved += 1
+                    vals[i] = old - float(np.sum(np.linalg.eigvalsh(A) ** -s))
+                e = int(ids[int(np.argmax(vals))])
+                contenders.append((len(ids), solved))
+        seq.append(e)
+        live[e] = False
+        _dense_add(M, int(cand[e, 0]), int(cand[e, 1]))
+    return dict(sequence=seq, contenders=contenders)
+
+
+def eval_prefix_multi(M0, cand, seq, targets):
+    """Exact prefix gains for several (obj, s) targets (exact.py:65-82)."""
+    M = np.array(M0, dtype=np.float64, copy=True)
+    lam = np.linalg.eigvalsh(M)
+    base = [frac_value(lam, s, o) for o, s in targets]
+    out = [[] for _ in targets]
+    for e in seq:
+        _dense_add(M, int(cand[e, 0]), int(cand[e, 1]))
+        lam = np.linalg.eigvalsh(M)
+        for i, (o, s) in enumerate(targets):
+            out[i].append(base[i] - frac_value(lam, s, o))
+    return [np.array(v) for v in out]
+
+
+def brute_force(M0, cand, k, s, obj="frac"):
+    """Best budget-k set by enumeration (exact.py:85-108); first maximum in
+    itertools.combinations order."""
+    import itertools
+    M = np.asarray(M0, dtype=np.float64)
+    base = frac_value(np.linalg.eigvalsh(M), s, obj)
+    best, arg = -np.inf, None
+    for C in itertools.combinations(range(len(cand)), k):
+        A = M.copy()
+        for j in C:
+            _dense_add(A, int(cand[j, 0]), int(cand[j, 1]))
+        g = base - frac_value(np.linalg.eigvalsh(A), s, obj)
+        if g > best:
+            best, arg = g, list(C)
+    return best, arg

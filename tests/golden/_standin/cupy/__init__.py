@@ -16,7 +16,12 @@ def asnumpy(a):
     return _np.asarray(a)
 
 
+ARGSORT_LOG = []
+
+
 def argsort(a, axis=-1, kind=None):
+    """Stable, as CuPy's; records each input so the generator can keep the proxy scores."""
+    ARGSORT_LOG.append(_np.array(a, copy=True))
     return _np.argsort(a, axis=axis, kind="stable")
 
 

@@ -104,3 +104,64 @@ def test_true_marginals_match_reference(gold):
         g, cert = O.true_marginals(G, cand, meta["tm_seq"], 0.5, obj=obj, eps=1e-4, tol=1e-10)
         np.testing.assert_allclose(g, z[f"tm_{obj}"], rtol=1e-9)
         assert cert["residual_rho"] == pytest.approx(float(z[f"tm_{obj}_rho"]))
+
+
+# ---------------------------------------------------------------------------------------
+# dense eigendecomposition oracles (realworld/exact.py) against the reference's outputs
+def _exact_case(key):
+    import json
+    z = np.load(GOLD / "reference_exact.npz")
+    meta = json.loads((GOLD / "reference_exact.json").read_text())
+    n = meta["exact_cases"][key][0]
+    E = z[f"ex_{key}_edges"]
+    M0 = O.Graph(n, E, 1e-2).M0.toarray()
+    return z, meta, M0, z[f"ex_{key}_cand"]
+
+
+@pytest.mark.parametrize("key", ["a", "b"])
+def test_exact_oracles_match_reference(key):
+    z, meta, M0, cand = _exact_case(key)
+    for obj, s in (("frac", 0.5), ("frac", 0.25), ("er", 1.0), ("logdet", 0.5)):
+        tag = f"{obj}{int(round(s * 100)):03d}"
+        r = O.exact_greedy(M0, cand, 4, s, obj=obj)
+        assert r["sequence"] == [int(x) for x in z[f"ex_{key}_{tag}_sequence"]]
+        if obj == "frac":
+            np.testing.assert_array_equal(np.array(r["contenders"]), z[f"ex_{key}_{tag}_contenders"])
+        pre = O.eval_prefix_multi(M0, cand, r["sequence"], [(obj, s)])[0]
+        np.testing.assert_allclose(pre, z[f"ex_{key}_{tag}_prefix"], rtol=1e-10)
+    seq = [int(x) for x in z[f"ex_{key}_frac050_sequence"]]
+    multi = O.eval_prefix_multi(M0, cand, seq, [tuple(t) for t in meta[f"ex_{key}_targets"]])
+    np.testing.assert_allclose(np.array(multi), z[f"ex_{key}_multi"], rtol=1e-10)
+    np.testing.assert_allclose(O.twin_gain(M0, cand, 0.5), z[f"ex_{key}_twin"], rtol=1e-12)
+    best, arg = O.brute_force(M0, cand[:24], 2, 0.5)
+    assert arg == [int(x) for x in z[f"ex_{key}_brute_arg"]]
+    assert best == pytest.approx(float(z[f"ex_{key}_brute_best"]), rel=1e-10)
+
+
+# ---------------------------------------------------------------------------------------
+# inputs of the workload-shaped golden cases (the greedy runs themselves are -m gpu tests)
+@pytest.mark.parametrize("name", ["s025", "s050", "s075", "plain_rad"])
+def test_mid_golden_inputs(name):
+    import json
+    from polar_b200.sketch import sketches
+    p = GOLD / f"reference_mid_{name}.npz"
+    if not p.exists():
+        pytest.skip("golden case not generated")
+    z = np.load(p)
+    c = json.loads((GOLD / f"reference_mid_{name}.json").read_text())[name]
+    pre = f"mid_{name}_"
+    if name == "plain_rad":
+        n, E = 2000, chung_lu(2000, 6.0, 2.5, 0, min_degree=1)
+        cand = candidates(n, E, 20000, 7919)
+    else:
+        n = 20000
+        E = chung_lu(n, 2 * 1049866 / 317080, 2.4, 1, min_degree=1)
+        cand = candidates(n, E, 20000, 1 + 7919)
+    assert (n, len(cand)) == (c["n"], c["N"])
+    assert int(E.sum()) == int(z[pre + "edges_sum"]) and len(E) == int(z[pre + "m"])
+    np.testing.assert_array_equal(cand[:64], z[pre + "cand_head"])
+    assert int(cand.sum()) == int(z[pre + "cand_sum"])
+    sk = sketches(O.Graph(n, E, 1e-2), cand, c["q"], 2026, kind=c["kind"])
+    np.testing.assert_allclose([float(np.sum(a)) for a in sk], z[pre + "sketch_sums"], rtol=1e-9, atol=1e-9)
+    assert z[pre + "shortlists"].shape == (c["k"], c["B"])
+    assert len(z[pre + "sequence"]) == c["k"]
