@@ -2,7 +2,14 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "polar.h"
+
 namespace polar {
+
+// polar_spmm's argument checks (everything but the scratch pointer) and the offset of its
+// heavy-row arrival counters inside the scratch; shared with polar_spmm_noalloc.
+int spmm_check_args(const polar_graph* g, int precision, int R, const void* d_X, int ldx, const void* d_Y, int ldy);
+size_t spmm_counter_offset(const polar_graph* g, int precision);
 
 int set_error(int code, const char* msg);
 int set_cuda_error(const char* what, cudaError_t e);

@@ -146,12 +146,30 @@ static int launch_spmm(const polar_graph& g, int R, double shift, const void* X,
 
 using namespace polar;
 
+namespace polar {
+
+size_t spmm_counter_offset(const polar_graph* g, int precision) {
+  const size_t es = precision == POLAR_MIXED ? 4 : 8;
+  return ((size_t)(g->nchunks > 0 ? g->nchunks : 1) * 128 * es + 255) & ~size_t(255);
+}
+
+int spmm_check_args(const polar_graph* g, int precision, int R, const void* d_X, int ldx, const void* d_Y,
+                    int ldy) {
+  if (!g || !d_X || !d_Y) return set_error(POLAR_ERR_BAD_ARG, "null pointer");
+  if (precision != POLAR_FP64 && precision != POLAR_MIXED) return set_error(POLAR_ERR_BAD_ARG, "precision");
+  if (R < 1 || ldx < R || ldy < R) return set_error(POLAR_ERR_BAD_ARG, "bad sizes");
+  const int vec = spmm_vec(precision, R, ldx, ldy, d_X, d_Y);
+  if ((R + vec - 1) / vec > 32) return set_error(POLAR_ERR_BAD_ARG, "R too large for one pass; split columns");
+  if ((g->d_wts == nullptr) != (g->d_diag == nullptr)) return set_error(POLAR_ERR_BAD_ARG, "weights and diag go together");
+  return POLAR_OK;
+}
+
+}  // namespace polar
+
 extern "C" size_t polar_spmm_scratch_bytes(const polar_graph* g, int precision, int R) {
   (void)R;
   if (!g) return 0;
-  const size_t es = precision == POLAR_MIXED ? 4 : 8;
-  const size_t part = (((size_t)(g->nchunks > 0 ? g->nchunks : 1) * 128 * es + 255) & ~size_t(255));
-  return part + (((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 * 8 + 255) & ~size_t(255));
+  return spmm_counter_offset(g, precision) + (((size_t)(g->nheavy > 0 ? g->nheavy : 1) * 4 * 8 + 255) & ~size_t(255));
 }
 
 extern "C" int polar_spmm_scratch_init(const polar_graph* g, int precision, int R, void* d_scratch,
@@ -166,11 +184,10 @@ extern "C" int polar_spmm_scratch_init(const polar_graph* g, int precision, int 
 extern "C" int polar_spmm(const polar_graph* g, int precision, int R, double shift, const void* d_X, int ldx,
                           void* d_Y, int ldy, void* d_scratch, polar_stream_t stream) {
   clear_error();
-  if (!g || !d_X || !d_Y || !d_scratch) return set_error(POLAR_ERR_BAD_ARG, "null pointer");
-  if (R < 1 || ldx < R || ldy < R) return set_error(POLAR_ERR_BAD_ARG, "bad sizes");
+  if (!d_scratch) return set_error(POLAR_ERR_BAD_ARG, "null pointer");
+  const int rc = spmm_check_args(g, precision, R, d_X, ldx, d_Y, ldy);
+  if (rc != POLAR_OK) return rc;
   const int vec = spmm_vec(precision, R, ldx, ldy, d_X, d_Y);
-  if ((R + vec - 1) / vec > 32) return set_error(POLAR_ERR_BAD_ARG, "R too large for one pass; split columns");
-  if ((g->d_wts == nullptr) != (g->d_diag == nullptr)) return set_error(POLAR_ERR_BAD_ARG, "weights and diag go together");
   const bool w = g->d_wts != nullptr;
   cudaStream_t st = (cudaStream_t)stream;
   const bool pow2 = (R & (R - 1)) == 0;

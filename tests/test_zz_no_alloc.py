@@ -58,3 +58,34 @@ def test_noalloc_rejects_oversize_scratch():
     assert rc == _lib.POLAR_ERR_WORKSPACE
     assert b"fixed" in lib.polar_last_error()
     assert lib.polar_launch_count() == before
+
+
+def test_noalloc_rejects_bad_arguments_before_queueing():
+    """Bad sizes and a weights/diagonal mismatch return BAD_ARG before the counter clear is
+    queued: a capture of the stream around the rejected calls holds no node."""
+    import torch
+    from cuda.bindings import runtime as rt
+    import polar_b200 as pg
+    from polar_b200 import _lib
+    lib = _lib.load()
+    n = 4000
+    G = pg.Graph(n, chung_lu(n, 6.0, 2.2, 9), 1e-2, heavy_thresh=8)
+    g = pg.Op(G).struct()
+    X = torch.zeros((n, 16), dtype=torch.float64, device="cuda")
+    Y = torch.zeros_like(X)
+    gw = pg.Op(G).struct()
+    gw.d_wts = X.data_ptr()  # weights without a diagonal
+    s = torch.cuda.Stream()
+    h = s.cuda_stream
+    (err,) = rt.cudaStreamBeginCapture(h, rt.cudaStreamCaptureMode.cudaStreamCaptureModeRelaxed)
+    assert err == rt.cudaError_t.cudaSuccess
+    rcs = [lib.polar_spmm_noalloc(ctypes.byref(g), _lib.POLAR_FP64, 0, 0.0, X.data_ptr(), 16, Y.data_ptr(), 16, h),
+           lib.polar_spmm_noalloc(ctypes.byref(g), _lib.POLAR_FP64, 16, 0.0, X.data_ptr(), 8, Y.data_ptr(), 16, h),
+           lib.polar_spmm_noalloc(ctypes.byref(g), 9, 16, 0.0, X.data_ptr(), 16, Y.data_ptr(), 16, h),
+           lib.polar_spmm_noalloc(ctypes.byref(gw), _lib.POLAR_FP64, 16, 0.0, X.data_ptr(), 16, Y.data_ptr(), 16, h)]
+    err, graph = rt.cudaStreamEndCapture(h)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, _, count = rt.cudaGraphGetNodes(graph, 0)
+    rt.cudaGraphDestroy(graph)
+    assert rcs == [_lib.POLAR_ERR_BAD_ARG] * 4
+    assert count == 0
