@@ -1,21 +1,29 @@
 """POLAR solve-and-score benchmark on B200.
 
-Workload (precision config): Chung–Lu n=317,080 (~1.05M edges, exponent 2.4, seed 1),
-sigma=1e-2, s=0.5, K=24 poles, q=64 sketch columns, N=200,000 candidate non-edges, B=16,
-k=50 rounds, CG tol 1e-7.  The seeded synthetic graph stands in for com-DBLP (same n and
-m; the SNAP file is not available here).
+Default workload (full-n4M): the full-scale greedy.  Chung–Lu n = 3,997,962 (34.7M edges,
+exponent 2.1, expected degree capped at 15,000, min degree 1, seed 4), sigma = 1e-2,
+s = 0.5, K = 32 poles, q = 64 sketch columns, N = 10^6 uniform non-edge candidates,
+B = 16, k = 100 rounds, CG tol 1e-6.  The seeded synthetic graph stands in for
+com-LiveJournal (same n and m; the SNAP file is not available here).
 
-One step = one complete k-round greedy POLAR run (bank solve, then per round: proxy score
-+ top-B, B-column shortlist solve, re-rank, maintenance).  `value` = mixed-precision
-greedy time (device events; inputs resident).  The FP64 path runs once beside it for
-parity (same sequence, max relative marginal error).  `e2e` times the public API
-(polar_b200.Graph + polar_b200.polar) from host arrays, uploads included.
+One step = one greedy round (realworld/polar_gpu.py:215-251): proxy scores of all N
+candidates and the stable top-B shortlist, the B-column multi-shift solve over all K poles,
+the re-rank, and the Sherman–Morrison maintenance of the 2q-column banks and h/t caches.
+The bank solve (2q = 128 right-hand sides, once per greedy) runs before the warm-up rounds
+and is timed separately; `greedy_s` = bank + k x value is the k-round greedy time.
+`value` = mixed-precision seconds per round (CUDA events around the K timed rounds; inputs
+resident in HBM).  The FP64 path runs the same rounds after it (`parity`: same sequence,
+max relative marginal error, FP64 seconds per round and bank, mixed-over-FP64 speed-up).
+`e2e` = polar_b200.Graph + polar_b200.Greedy from host arrays (edge list, candidates and
+sketch arrays uploaded, bank, K rounds, winners read back), wall clock divided by K.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--impl reference]
+    python bench.py --config full-n4M --solve [--quick]   # one shortlist solve, kernel table
+    python bench.py --config batch48                      # many graphs in one call
 
-Multi-GPU: the greedy does not shard (one graph per greedy); N GPUs run N independent
-replicas on graphs of different seeds, with no collective on the data path; value is
-the mean greedy time of the replicas (max over ranks of the device time / K).
+Multi-GPU: one greedy is one graph and does not shard here; N GPUs run N independent
+replicas (sketch seeds 2026 + 1000 rank), no collective on the data path; value is the
+mean round time of the replicas (max over ranks of the device time / K).
 """
 import argparse
 import json
@@ -30,8 +38,9 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "k-round greedy time (mixed precision, FP64 parity)"
-UNIT = "s/greedy"
+METRIC = "greedy round time, mixed precision (FP64 parity beside)"
+UNIT = "s/round"
+ITER_FILE = os.path.join(ROOT, "profiles", "iterations_per_round.json")
 
 
 def parse():
@@ -40,18 +49,20 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="precision-n317k")
+    ap.add_argument("--config", default="full-n4M")
     ap.add_argument("--n", type=int, default=None, help="shrink the graph (debug)")
     ap.add_argument("--N", type=int, default=None)
     ap.add_argument("--k", type=int, default=None)
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-iters", type=int, default=1, help="oracle CG iterations timed per width")
-    ap.add_argument("--phases", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true", help="keep the solver's default SpMM layouts")
-    ap.add_argument("--quick", action="store_true", help="full-n4M: one short solve (an ncu-sized case)")
-    ap.add_argument("--cache", default=None, help="full-n4M: .npz file holding the generated edge list "
-                                                    "(written when absent, read when present)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=2, help="oracle CG iterations timed for the CPU baseline")
+    ap.add_argument("--autotune", default="auto", choices=["auto", "on", "off"],
+                    help="SpMM layout tuning of the shortlist width (auto: graphs under 2M vertices)")
+    ap.add_argument("--l2", default=None, help="L2 policy MODE:MB for the solver (polar_set_l2_policy)")
+    ap.add_argument("--solve", action="store_true", help="one shortlist solve with its kernel table")
+    ap.add_argument("--quick", action="store_true", help="--solve: 48-iteration solves (an ncu-sized case)")
+    ap.add_argument("--cache", default=None, help="directory for generated workloads (.npz, reused when present)")
     return ap.parse_args()
 
 
@@ -118,7 +129,8 @@ def peak_hbm():
 
 
 def profiled_traffic(config):
-    """DRAM bytes per SpMM launch from the committed ncu summary (null when absent)."""
+    """DRAM bytes per shortlist-solve SpMM launch from the committed ncu summary (null when
+    absent)."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if not os.path.exists(p):
         return None
@@ -129,7 +141,7 @@ def profiled_traffic(config):
 
 # ---------------------------------------------------------------------------------------
 def replica_seed(base_seed, rank):
-    """Seed of rank `rank`'s replica graph: replicas run independent greedies."""
+    """Sketch seed of rank `rank`'s replica: replicas run independent greedies."""
     return base_seed + 1000 * rank
 
 
@@ -146,54 +158,120 @@ def job_seconds(local_s, world, device):
     return float(t.item())
 
 
-def build_inputs(a, rank=0):
+def build_inputs(a):
+    """(n, N, k, edges, candidates, config) of the workload, generated from its seeds (or
+    read from --cache, where a previous run left them)."""
     from polar_b200.synth import CONFIGS, candidates, chung_lu
     c = dict(CONFIGS[a.config])
     n = a.n or c["n"]
     N = a.N or c["N"]
     k = a.k or c["k"]
-    seed = replica_seed(c["seed"], rank)
-    E = chung_lu(n, c["mean_deg"], c["gamma"], seed, dmax=c["dmax"] if n == c["n"] else None,
+    path = None
+    if a.cache:
+        os.makedirs(a.cache, exist_ok=True)
+        path = os.path.join(a.cache, f"{a.config}_n{n}_N{N}.npz")
+        if os.path.exists(path):
+            z = np.load(path)
+            return dict(n=n, N=N, k=k, E=z["edges"].astype(np.int64), cand=z["cand"].astype(np.int64), cfg=c)
+    E = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=c["dmax"] if n == c["n"] else None,
                  min_degree=c.get("min_degree", 0))
-    cand = candidates(n, E, N, seed + 7919)
-    return dict(n=n, N=N, k=k, E=E, cand=cand, cfg=c, seed=seed)
+    cand = candidates(n, E, N, c["seed"] + 7919)
+    if path:
+        np.savez(path, edges=E.astype(np.int32), cand=cand.astype(np.int32))
+    return dict(n=n, N=N, k=k, E=E, cand=cand, cfg=c)
 
 
-def oracle_iteration_costs(inp, sk, tau, active_h, widths, iters):
-    """Seconds per multi-shift CG iteration of the oracle (NumPy FP64, the host's BLAS
-    threads) at each column width, from `iters` timed iterations."""
+# ---------------------------------------------------------------------------------------
+# CPU side: the reference's algorithm on the host cores, through the oracle (a NumPy FP64
+# restatement of realworld/polar_gpu.py).  A round of the full-scale workload takes hours
+# there, so a bounded sample is timed for real and scaled by the round's iteration count:
+#   s/round = (s per multi-shift CG iteration at B columns) x (seed iterations per round)
+#           + (proxy scores and stable top-B over N) + (Sherman–Morrison maintenance)
+def oracle_round_parts(inp, iters, warm=1, on_sample=None):
+    """Times `iters` multi-shift CG iterations of the oracle on a B-column shortlist solve
+    of the workload (full graph, all K poles, all active rows; right-hand sides = the
+    incidence vectors of B candidate edges), plus the per-round scoring and maintenance.
+    Returns dict(iteration_s list, score_s, maintain_s, sample_s)."""
+    import polar_b200.quadrature as Q
     from oracle import polar_oracle as O
+    t_all = time.perf_counter()
     c = inp["cfg"]
-    op = O.Op(O.Graph(inp["n"], inp["E"], c["sigma"]))
-    out = {}
-    rhs = np.concatenate([sk[0], sk[1]], axis=1)
-    for w in widths:
-        W = rhs[:, :w] if w <= rhs.shape[1] else np.tile(rhs, (1, -(-w // rhs.shape[1])))[:, :w]
-        t0 = time.perf_counter()
-        try:
-            O.msolve(op, W, tau, active_h, 1e-30, maxit=iters)
-        except RuntimeError:
-            pass
-        out[w] = (time.perf_counter() - t0) / iters
-    return out
+    n, cand = inp["n"], inp["cand"]
+    OG = O.Graph(n, inp["E"], c["sigma"])
+    tau, om, _ = Q.poles("frac", c["s"], c["sigma"], OG.Lam(inp["k"]), 1e-2, K=c["K"])
+    active = np.unique(cand)
+    B = c["B"]
+    W = np.zeros((n, B))
+    W[cand[:B, 0], np.arange(B)] = 1.0
+    W[cand[:B, 1], np.arange(B)] = -1.0
+    times = []
+    last = [time.perf_counter()]
+
+    def tick(it):
+        now = time.perf_counter()
+        times.append(now - last[0])
+        last[0] = now
+        if on_sample is not None and len(times) > warm:
+            on_sample(len(times) - warm - 1, times[-1])
+
+    try:
+        O.msolve(O.Op(OG), W, tau, active, 1e-300, maxit=iters + warm, on_iteration=tick)
+    except RuntimeError:
+        pass  # the iteration cap ends the sample
+    # scoring over all N candidates and the stable top-B (polar_gpu.py:219-221)
+    p, N = len(tau), len(cand)
+    rng = np.random.default_rng(0)
+    h = rng.random((p, N))
+    t = rng.random((p, N))
+    t0 = time.perf_counter()
+    sc = O.proxy_scores(h, t, om, tau, c["sigma"])
+    np.argsort(-sc, kind="stable")[:B]
+    score_s = time.perf_counter() - t0
+    # maintenance on 1/16 of the active rows, scaled by 16 (its cost is linear in rows)
+    nA = len(active)
+    ns = max(2, nA // 16)
+    q = c["q"]
+    X = rng.normal(size=(p, ns, q))
+    Y = rng.normal(size=(p, ns, q))
+    u = rng.normal(size=(p, ns)) * 1e-3
+    es = np.searchsorted(active, cand) % ns
+    t0 = time.perf_counter()
+    O.maintain(X, Y, h, t, u, rng.normal(size=q), 0, 1, es[:, 0], es[:, 1])
+    maintain_s = (time.perf_counter() - t0) * (nA / ns)
+    return dict(iteration_s=times[warm:], score_s=score_s, maintain_s=maintain_s, p=p, nA=nA,
+                sample_s=time.perf_counter() - t_all)
 
 
-def cpu_estimate(costs, solves, oracle_width=64):
-    """Greedy seconds of the oracle for these solves: the oracle runs the bank in chunks
-    of `oracle_width` columns (realworld/polar_gpu.py:169-173) and one shortlist solve per
-    round; per-iteration cost is interpolated linearly in the column count."""
-    ws = sorted(costs)
-    t_at = lambda R: float(np.interp(R, ws, [costs[w] for w in ws]))
-    total = 0.0
-    for R, it in solves:
-        if R > oracle_width:
-            total += (R // oracle_width) * t_at(oracle_width) * it
-        else:
-            total += t_at(R) * it
-    return total
+def committed_iterations(config):
+    """Seed iterations of each round's shortlist solve and of the bank, from the FP64 GPU run
+    recorded in profiles/iterations_per_round.json (the iteration count is a property of the
+    linear systems: the FP64 GPU path matches the reference's own counts within 2)."""
+    if not os.path.exists(ITER_FILE):
+        return None
+    with open(ITER_FILE) as f:
+        return json.load(f).get(config)
 
 
-def run_ours(a):
+def cpu_round_estimate(parts, rounds_iters, bank_iters, k, q):
+    """s/round and k-round greedy seconds of the oracle from timed parts."""
+    it_s = float(np.mean(parts["iteration_s"]))
+    per_round = it_s * float(np.mean(rounds_iters)) + parts["score_s"] + parts["maintain_s"]
+    # the reference solves the bank in chunks of chunk_width columns (16 above 3e6 rows,
+    # realworld/polar_gpu.py:169-173), each costing about a B = 16 iteration per iteration
+    bank_s = it_s * bank_iters * (2 * q / 16)
+    return per_round, bank_s + k * per_round, it_s
+
+
+# ---------------------------------------------------------------------------------------
+def release_device_memory():
+    import torch
+    from polar_b200 import solver as S
+    S._WS.clear()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+
+def run_greedy(a):
     import torch
     import torch.distributed as dist
 
@@ -209,61 +287,93 @@ def run_ours(a):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900), device_id=dev)
     lib = _lib.load()
-    inp = build_inputs(a, rank)
+    if a.l2:
+        mode, mb = a.l2.split(":")
+        _lib.check(lib.polar_set_l2_policy(int(mode), int(float(mb) * (1 << 20))), "l2 policy")
+    t_setup = time.perf_counter()
+    inp = build_inputs(a)
     n, N, k, E, cand, c = inp["n"], inp["N"], inp["k"], inp["E"], inp["cand"], inp["cfg"]
+    rounds = a.warmup + a.steps
+    if rounds + 1 > k:
+        raise SystemExit(f"warm-up + steps + 1 instrumented round = {rounds + 1} exceeds the workload's k = {k}")
+    t_gen = time.perf_counter() - t_setup
     G = pg.Graph(n, E, c["sigma"])
-    sk = pg.sketches(G, cand, c["q"], 2026)
+    sk = pg.sketches(G, cand, c["q"], replica_seed(2026, rank), device=True)
     kw = dict(q=c["q"], B=c["B"], tol=c["tol"], sketch=sk, K=c["K"])
     tuned = {}
-    if not a.no_autotune:
-        # SpMM layout per solve width (shortlist B, bank 2q), timed once before any greedy
+    if a.autotune == "on" or (a.autotune == "auto" and n < 2_000_000):
+        # SpMM layout of the shortlist width, timed once before any greedy
         from polar_b200 import autotune
-        for prec, wide in (("mixed", 128),) + ((("fp64", 64),) if not a.no_fp64 else ()):
-            for R in sorted({c["B"], min(2 * c["q"], wide)}):
-                t = autotune.tune_msolve(pg.Op(G), R, prec, p=c["K"])
-                tuned[f"{prec}_R{R}"] = {"lane_bytes": t["best"][0], "sliced_ell": t["best"][1],
-                                         "heavy_thresh": t["best"][2], "us_per_iter": t["us_per_iter"],
-                                         "layouts_timed": len(t["table"])}
+        for prec in ("mixed",) + (("fp64",) if not a.no_fp64 else ()):
+            t = autotune.tune_msolve(pg.Op(G), c["B"], prec, p=c["K"])
+            tuned[f"{prec}_R{c['B']}"] = {"lane_bytes": t["best"][0], "sliced_ell": t["best"][1],
+                                          "heavy_thresh": t["best"][2], "us_per_iter": t["us_per_iter"],
+                                          "layouts_timed": len(t["table"])}
+    setup_s = time.perf_counter() - t_setup
 
-    def timed_run(prec, **extra):
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        res = pg.polar(G, cand, k, c["s"], precision=prec, **kw, **extra)
-        e1.record()
-        torch.cuda.synchronize()
-        res["device_s"] = e0.elapsed_time(e1) / 1e3
-        return res
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
 
-    fp64 = None if a.no_fp64 else timed_run("fp64")
+    def banked(prec):
+        g = pg.Greedy(G, cand, k, c["s"], precision=prec, **kw)
+        torch.cuda.synchronize()
+        b0, b1 = ev(), ev()
+        b0.record()
+        g.bank()
+        b1.record()
+        torch.cuda.synchronize()
+        return g, b0.elapsed_time(b1) / 1e3
+
+    # ---- mixed precision: bank, warm-up rounds, then exactly K timed rounds ----
+    g, bank_s = banked("mixed")
     for _ in range(a.warmup):
-        mixed = timed_run("mixed")
-
-    # ---- timed region: exactly K greedy runs, uninstrumented ----
+        g.step()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = lib.polar_launch_count()
     with Clocks(local) as clk:
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record()
-        runs = [pg.polar(G, cand, k, c["s"], precision="mixed", phases=a.phases, **kw) for _ in range(a.steps)]
-        ev1.record()
+        e0, e1 = ev(), ev()
+        e0.record()
+        for _ in range(a.steps):
+            g.step()
+        e1.record()
         torch.cuda.synchronize()
     launches = lib.polar_launch_count() - launches0
-    total_s = job_seconds(ev0.elapsed_time(ev1) / 1e3, world, dev)
-    # ---- one more greedy with every solver kernel bracketed by CUDA events (the event
-    # nodes serialise the iteration graph, so this run is not part of `value`) ----
-    torch.cuda.synchronize()
+    total_s = job_seconds(e0.elapsed_time(e1) / 1e3, world, dev)
+    per = total_s / a.steps
+    # ---- one more round with every solver kernel bracketed by CUDA events (the event
+    # nodes serialise the iteration graph, so this round is not part of `value`) ----
     lib.polar_set_kernel_timing(1)
-    inst = timed_run("mixed")
+    i0, i1 = ev(), ev()
+    i0.record()
+    g.step()
+    i1.record()
+    torch.cuda.synchronize()
     ktime = _lib.kernel_timing()
     lib.polar_set_kernel_timing(0)
-    per = total_s / a.steps
-    mixed = runs[-1]
+    inst_s = i0.elapsed_time(i1) / 1e3
+    mixed = g.result()
+    del g
+    release_device_memory()
 
-    # ---- roofline of the dominant kernel (the SpMM of the multi-shift CG: heavy-row and
-    # light-row launches together; algorithmic bytes are counted on the light class) ----
+    # ---- FP64: the same rounds ----
+    fp64 = None
+    if not a.no_fp64:
+        g, bank64_s = banked("fp64")
+        t64 = []
+        for _ in range(rounds + 1):
+            r0, r1 = ev(), ev()
+            r0.record()
+            g.step()
+            r1.record()
+            torch.cuda.synchronize()
+            t64.append(r0.elapsed_time(r1) / 1e3)
+        fp64 = dict(g.result(), bank_s=bank64_s, round_s=t64)
+        del g
+        release_device_memory()
+
+    # ---- roofline of the dominant kernel: the SpMM of the shortlist solves ----
     hbm, peak_kind = peak_hbm()
     nl, ms_l, by = ktime["spmm"]
     ms = ms_l + ktime["spmm_heavy"][1]
@@ -276,15 +386,24 @@ def run_ours(a):
         kernels[name]["share"] = ktime[name][1] / ktot if ktot else None
 
     # ---- end to end through the public API, from host arrays ----
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    G2 = pg.Graph(n, E, c["sigma"])
-    res_e2e = pg.polar(G2, cand, k, c["s"], precision="mixed", **kw)
-    _ = list(res_e2e["sequence"])
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    h2d = E.nbytes + cand.nbytes + sum(np.asarray(x).nbytes for x in sk)
-    d2h = 8 * 6 * k + 8 * 2 * k
+    e2e = None
+    if not a.no_e2e:
+        sk_h = [x.cpu().numpy() for x in sk]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        G2 = pg.Graph(n, E, c["sigma"])
+        g2 = pg.Greedy(G2, cand, k, c["s"], q=c["q"], B=c["B"], tol=c["tol"], sketch=sk_h, K=c["K"],
+                       precision="mixed")
+        seq2 = [g2.step() for _ in range(a.steps)]
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t0) / a.steps
+        h2d = E.nbytes + cand.nbytes + sum(x.nbytes for x in sk_h)
+        e2e = {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d / a.steps),
+               "d2h_bytes_per_step": int(8 * 6 + 8 * 2),
+               "note": "Graph + Greedy from host arrays: uploads, bank and %d rounds, wall clock / %d"
+                       % (a.steps, a.steps), "same_sequence": seq2 == mixed["sequence"][:a.steps]}
+        del g2, G2, sk_h
+        release_device_memory()
 
     parity = {}
     if fp64 is not None:
@@ -293,56 +412,73 @@ def run_ours(a):
         same = fp64["sequence"] == mixed["sequence"]
         upto = len(mf) if same else next(i for i, (x, y) in enumerate(zip(fp64["sequence"], mixed["sequence"]))
                                          if x != y)
+        per64 = float(np.sum(fp64["round_s"][a.warmup:rounds]) / a.steps)
         parity = {"same_sequence": same, "rounds_compared": upto,
                   "max_rel_marginal_err": float(np.max(np.abs(mm[:upto] - mf[:upto]) / np.abs(mf[:upto])))
                   if upto else None,
-                  "fp64_greedy_s": fp64["device_s"], "mixed_speedup_vs_fp64": fp64["device_s"] / per}
+                  "fp64_round_s": per64, "fp64_bank_s": fp64["bank_s"],
+                  "fp64_greedy_s": fp64["bank_s"] + k * per64,
+                  "mixed_speedup_vs_fp64": (fp64["bank_s"] + k * per64) / (bank_s + k * per),
+                  "mixed_round_speedup_vs_fp64": per64 / per}
+
+    def shortlist_iters(res):
+        return [it for R, it in res["solves"] if R == c["B"]]
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
-        tau, _, _ = pg.poles("frac", c["s"], c["sigma"], G.Lam(k), 1e-2, K=c["K"])
-        costs = oracle_iteration_costs(inp, sk, tau, np.unique(cand), (64, c["B"]), a.cpu_iters)
-        est = cpu_estimate(costs, mixed["solves"])
-        cpu = {"value": est, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-               "sample": (f"oracle (NumPy FP64 restatement of polar_gpu.py) multi-shift CG timed for "
-                          f"{a.cpu_iters} iteration(s) at 64 and {c['B']} columns "
-                          f"({costs[64]:.2f} / {costs[c['B']]:.2f} s per iteration, BLAS on all host threads, "
-                          f"SciPy SpMM on 1 core), times this greedy's seed iterations per solve "
-                          f"({sum(it for _, it in mixed['solves'])} iterations over {len(mixed['solves'])} solves)")}
+        parts = oracle_round_parts(inp, a.cpu_iters)
+        ref_iters = shortlist_iters(fp64 if fp64 is not None else mixed)
+        bank_iters = max(it for R, it in (fp64 or mixed)["solves"] if R != c["B"])
+        est, greedy_est, it_s = cpu_round_estimate(parts, ref_iters, bank_iters, k, c["q"])
+        cpu = {"value": est, "unit": UNIT, "cores": 1, "kind": "port",
+               "greedy_s": greedy_est,
+               "sample": (f"oracle (NumPy FP64 restatement of polar_gpu.py) multi-shift CG on this workload's "
+                          f"shortlist solve ({c['B']} columns, {parts['p']} poles, {parts['nA']} active rows): "
+                          f"{len(parts['iteration_s'])} timed iterations, {it_s:.2f} s each, x "
+                          f"{np.mean(ref_iters):.0f} seed iterations per round (this run's "
+                          f"{'FP64' if fp64 is not None else 'mixed'} solves) + scoring {parts['score_s']:.2f} s + "
+                          f"maintenance {parts['maintain_s']:.2f} s (timed on 1/16 of the rows); NumPy elementwise "
+                          f"and SciPy SpMM run on one core; {parts['sample_s']:.0f} s of host work")}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": per, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": per * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 SpMM input/output and pole iterates; f64 residual, direction and scalars",
-            "data": "synthetic (seeded Chung-Lu stand-in for com-DBLP shape)",
+            "data": "synthetic (seeded Chung-Lu stand-in for the %s shape)" % (
+                "com-LiveJournal" if a.config == "full-n4M" else a.config),
             "config": {"workload": a.config, "n": n, "m": int(len(E)), "N": N, "K": c["K"], "q": c["q"],
                        "B": c["B"], "k": k, "s": c["s"], "sigma": c["sigma"], "tol": c["tol"],
-                       "l2": "inputs larger than L2 (X/Y banks 2.8 GB, SpMM block 162 MB)",
+                       "step": "one greedy round",
+                       "l2": "inputs larger than L2 (X/Y banks %.1f GB, SpMM block %.0f MB)"
+                             % (mixed["p"] * len(np.unique(cand)) * 2 * c["q"] * 4 / 1e9, n * c["B"] * 4 / 1e6),
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "bank_s": bank_s, "greedy_s": bank_s + k * per,
+            "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm if achieved else None,
                          "traffic": profiled_traffic(a.config),
-                         "kernel": "mk_spmm (CSR SpMM + d.v of the multi-shift CG, heavy + light launches)",
+                         "kernel": "mk_spmm (SpMM + d.v of the shortlist multi-shift CG, R = %d)" % c["B"],
                          "peak_source": peak_kind, "launches": nl, "avg_launch_us": ms * 1e3 / nl if nl else None,
-                         "measured": "CUDA events around every solver kernel in one instrumented greedy run "
-                                     "right after the timed region (%.3f s with events)" % inst["device_s"]},
+                         "measured": "CUDA events around every solver kernel in one instrumented round right "
+                                     "after the timed region (%.3f s with events)" % inst_s},
             "kernels": kernels,
             "iteration_alg_GBps": (sum(v[2] for v in ktime.values()) / (ktot / 1e3) / 1e9) if ktot else None,
             "parity": parity,
             "sequence_head": mixed["sequence"][:8],
-            "spmv": mixed["spmv"], "p": mixed["p"],
-            "cg": {"seed_iterations": int(sum(it for _, it in mixed["solves"])), "column_iterations": mixed["spmv"],
-                   "seed_iterations_per_s": sum(it for _, it in mixed["solves"]) / per,
-                   "column_iterations_per_s": mixed["spmv"] / per},
+            "p": mixed["p"],
+            "iterations": {"bank": [it for R, it in mixed["solves"] if R != c["B"]],
+                           "mixed_per_round": shortlist_iters(mixed),
+                           "fp64_per_round": shortlist_iters(fp64) if fp64 else None,
+                           "fp64_bank": [it for R, it in fp64["solves"] if R != c["B"]] if fp64 else None},
+            "cg": {"seed_iterations_per_s": float(np.mean(shortlist_iters(mixed)[a.warmup:rounds])) / per,
+                   "column_iterations_per_s": float(np.mean(shortlist_iters(mixed)[a.warmup:rounds])) * c["B"] / per},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "autotune": tuned or None,
+            "host_setup_s": setup_s, "input_generation_s": t_gen,
         }
-        if a.phases:
-            line["phases"] = mixed.get("phases")
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -441,56 +577,46 @@ def run_batch(a):
     print(json.dumps(line), flush=True)
 
 
-def run_full(a):
-    """Full-scale solve: the shortlist solve of the n = 4.0M / 34.7M-edge workload (B = 16
-    incidence columns, K = 32 poles, tol 1e-6, pole iterates on ~1.57M active rows) in FP64
-    and in mixed precision, with the per-kernel table of each; plus the SpMM alone at 16 and
-    64 columns.  `--quick` runs only a 48-iteration mixed solve over 32 active rows (the
-    small case for an ncu capture of the SpMM)."""
+def run_solve(a):
+    """One shortlist solve of the workload (B incidence columns, all K poles, pole iterates
+    on the endpoints of all N candidates) in FP64 and in mixed precision, each with its
+    per-kernel table, plus the SpMM alone (polar_spmm through Op) at B and 4B columns.
+    --quick: 48-iteration mixed solves at B and 8B columns (the bank width) for every L2
+    policy in --l2 (comma-separated MODE:MB; default 0:0,1:64), printing the SpMM time per
+    launch; this is also the small case for an ncu capture of the SpMM."""
     import torch
 
     import polar_b200 as pg
     from polar_b200 import _lib
-    from polar_b200.synth import CONFIGS, candidates, chung_lu
+    from polar_b200 import solver as S
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
     lib = _lib.load()
-    c = CONFIGS["full-n4M"]
-    n = a.n or c["n"]
     t_gen = time.perf_counter()
-    if a.cache and os.path.exists(a.cache):
-        E = np.load(a.cache)["edges"].astype(np.int64)
-    else:
-        E = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=c["dmax"] if n == c["n"] else None,
-                     min_degree=c["min_degree"])
-        if a.cache:
-            np.savez(a.cache, edges=E.astype(np.int32))
-    pairs = candidates(n, E, c["B"], c["seed"] + 7919)
-    rng = np.random.default_rng(c["seed"])
-    # endpoints of N uniform candidate pairs: the active rows of the workload's pole iterates
-    Nq = 16 if a.quick else c["N"]
-    active = np.unique(np.concatenate([rng.integers(0, n, 2 * Nq), pairs.ravel()]))
+    inp = build_inputs(a)
+    n, E, cand, c = inp["n"], inp["E"], inp["cand"], inp["cfg"]
     G = pg.Graph(n, E, c["sigma"])
     t_gen = time.perf_counter() - t_gen
     op = pg.Op(G)
-    tau, om, _ = pg.poles("frac", c["s"], c["sigma"], G.Lam(c["k"]), 1e-2, K=c["K"])
+    tau, om, _ = pg.poles("frac", c["s"], c["sigma"], G.Lam(inp["k"]), 1e-2, K=c["K"])
     R = c["B"]
+    pairs = cand[:R]
+    active = np.unique(cand)
     W = np.zeros((n, R))
     W[pairs[:, 0], np.arange(R)] = 1.0
     W[pairs[:, 1], np.arange(R)] = -1.0
     Wd = torch.as_tensor(W).to(dev)
-    from polar_b200 import solver as S
     act_d, pos_d = S.prepare_active(active, n, dev)
     ia = np.searchsorted(active, pairs[:, 0])
     ib = np.searchsorted(active, pairs[:, 1])
 
-    def solve(prec, maxit=100000):
+    def solve(prec, Wm, maxit=100000, act=(act_d, pos_d)):
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         try:
-            X, h, it = S.msolve(op, Wd, tau, act_d, c["tol"], maxit=maxit, track=True, precision=prec,
-                                active_pos=pos_d)
+            X, h, it = S.msolve(op, Wm, tau, act[0], c["tol"], maxit=maxit, track=True, precision=prec,
+                                active_pos=act[1])
         except _lib.PolarError as e:
             if e.status != _lib.POLAR_ERR_ITER_CAP or maxit == 100000:
                 raise
@@ -500,35 +626,56 @@ def run_full(a):
         cols = torch.arange(R, device=dev)
         bu = (X[:, torch.as_tensor(ia, device=dev), cols].double()
               - X[:, torch.as_tensor(ib, device=dev), cols].double()).cpu().numpy()
-        G_q = (om[:, None] * h.cpu().numpy() / (1.0 + bu)).sum(0)
+        G_q = (om[:, None] * h[:, :R].cpu().numpy() / (1.0 + bu)).sum(0)
         return {"seconds": e0.elapsed_time(e1) / 1e3, "iterations": int(it.max()), "G": G_q}
 
     if a.quick:
-        lib.polar_set_kernel_timing(1)
-        solve("mixed", maxit=48)
-        kt = _lib.kernel_timing()
-        lib.polar_set_kernel_timing(0)
-        print(json.dumps({"workload": "full-n4M", "quick": True, "n": n, "nnz": G.nnz,
-                          "spmm_ms_per_launch": kt["spmm"][1] / max(1, kt["spmm"][0])}), flush=True)
+        # small pole state (active rows: the B pairs' endpoints) and full-height blocks
+        small = S.prepare_active(np.unique(pairs), n, dev)
+        ia = np.searchsorted(np.unique(pairs), pairs[:, 0])
+        ib = np.searchsorted(np.unique(pairs), pairs[:, 1])
+        W8 = torch.cat([Wd] * 8, dim=1) + 1e-3 * torch.randn((n, 8 * R), device=dev, dtype=torch.float64)
+        out = {}
+        for pol in (a.l2 or "0:0,1:64").split(","):
+            mode, mb = pol.split(":")
+            _lib.check(lib.polar_set_l2_policy(int(mode), int(float(mb) * (1 << 20))), "l2 policy")
+            row = {}
+            for name, Wm in (("R%d" % R, Wd), ("R%d" % (8 * R), W8)):
+                for prec in ("mixed", "fp64"):
+                    if prec == "fp64" and Wm.shape[1] > 64:
+                        continue
+                    lib.polar_set_kernel_timing(1)
+                    try:
+                        S.msolve(op, Wm, tau, small[0], c["tol"], maxit=48, track=False, precision=prec,
+                                 active_pos=small[1])
+                    except _lib.PolarError as e:
+                        if e.status != _lib.POLAR_ERR_ITER_CAP:
+                            raise
+                    kt = _lib.kernel_timing()
+                    lib.polar_set_kernel_timing(0)
+                    row[f"{prec}_{name}"] = {k2: round(v[1] / max(1, v[0]), 4) for k2, v in kt.items() if v[0]}
+            out[pol] = row
+        _lib.check(lib.polar_set_l2_policy(0, 64 << 20), "l2 policy")
+        print(json.dumps({"workload": a.config, "quick": True, "n": n, "nnz": G.nnz,
+                          "ms_per_launch_by_l2_policy": out}), flush=True)
         return
     out = {}
     for prec in ("fp64", "mixed"):
-        solve(prec, maxit=16)  # warm-up: graph partitions, workspace, CUDA graphs
-        res = solve(prec)
+        solve(prec, Wd, maxit=16)  # warm-up: graph partitions, workspace, CUDA graphs
+        res = solve(prec, Wd)
         lib.polar_set_kernel_timing(1)
-        inst = solve(prec)
+        inst = solve(prec, Wd)
         kt = _lib.kernel_timing()
         lib.polar_set_kernel_timing(0)
-        out[prec] = dict(res, kernels={k: {"launches": v[0], "ms": v[1],
-                                           "alg_GBps": v[2] / (v[1] / 1e3) / 1e9 if v[1] > 0 else None}
-                                       for k, v in kt.items() if v[0]},
+        out[prec] = dict(res, kernels={k2: {"launches": v[0], "ms": v[1],
+                                            "alg_GBps": v[2] / (v[1] / 1e3) / 1e9 if v[1] > 0 else None}
+                                       for k2, v in kt.items() if v[0]},
                          instrumented_seconds=inst["seconds"])
     G64, G32 = out["fp64"].pop("G"), out["mixed"].pop("G")
-    # the SpMM alone (polar_spmm through Op), 16 and 64 columns, both precisions
     hbm, peak_kind = peak_hbm()
     spmm = {}
     for dt, nm in ((torch.float64, "fp64"), (torch.float32, "mixed")):
-        for Rc in (16, 64):
+        for Rc in (R, 4 * R):
             Xs = torch.randn((n, Rc), device=dev, dtype=torch.float64).to(dt)
             op(Xs, 0.0)
             torch.cuda.synchronize()
@@ -545,9 +692,9 @@ def run_full(a):
             spmm[f"{nm}_R{Rc}"] = {"ms": ms, "alg_GBps": alg / (ms / 1e3) / 1e9,
                                    "frac_of_peak": alg / (ms / 1e3) / 1e9 / hbm}
             del Xs
-    line = {"metric": "full-scale shortlist solve (B = 16 columns, K = 32 poles)", "unit": "s/solve",
+    line = {"metric": "shortlist solve (B columns, K poles)", "unit": "s/solve",
             "value": out["mixed"]["seconds"], "higher_is_better": False, "n_gpus": 1,
-            "config": {"workload": "full-n4M", "n": n, "m": int(len(E)), "nnz": G.nnz, "dmax": G.dmax,
+            "config": {"workload": a.config, "n": n, "m": int(len(E)), "nnz": G.nnz, "dmax": G.dmax,
                        "nA": int(len(active)), "K": c["K"], "R": R, "tol": c["tol"], "sigma": c["sigma"], "s": c["s"]},
             "fp64": out["fp64"], "mixed": out["mixed"],
             "mixed_speedup_vs_fp64": out["fp64"]["seconds"] / out["mixed"]["seconds"],
@@ -557,83 +704,56 @@ def run_full(a):
 
 
 def run_reference(a):
-    """The reference's algorithm on the host: the oracle (a NumPy FP64 restatement of
-    realworld/polar_gpu.py; the reference itself needs CuPy and a GPU).  Per-iteration
-    cost is timed at the bank and shortlist widths; iteration counts come from seed-CG
-    runs of a sample of bank columns and shortlist edges (SciPy, FP64)."""
+    """The reference's algorithm on the host cores for the same workload and metric: the
+    oracle (a NumPy FP64 restatement of realworld/polar_gpu.py, pinned to the reference's
+    own outputs; the reference itself needs CuPy and a GPU).  Each step is one timed
+    multi-shift CG iteration of the workload's shortlist solve (B columns, all K poles, all
+    active rows, full graph); value = s per iteration x the seed iterations of a round (the
+    FP64 GPU path's per-round counts, profiles/iterations_per_round.json) + the per-round
+    scoring and maintenance, timed once.  Rank 0 alone runs; other ranks exit."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import polar_b200.quadrature as Q
-    from oracle import polar_oracle as O
-    inp = build_inputs(a, 0)
+    rec = committed_iterations(a.config)
+    if rec is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no recorded per-round iteration counts for "
+                          f"{a.config} in profiles/iterations_per_round.json"}), flush=True)
+        return
+    inp = build_inputs(a)
     c = inp["cfg"]
-    OG = O.Graph(inp["n"], inp["E"], c["sigma"])
-    sk = O.sketches(OG, inp["cand"], c["q"], 2026)
-    tau, _, _ = Q.poles("frac", c["s"], c["sigma"], OG.Lam(inp["k"]), 1e-2, K=c["K"])
-    active_h = np.unique(inp["cand"])
-    n = inp["n"]
-
-    def seed_iters(w):
-        A = OG.M0 + tau[0] * __import__("scipy.sparse", fromlist=["eye"]).eye(n, format="csr")
-        r = w.copy()
-        d = r.copy()
-        rr = r @ r
-        stop = c["tol"] * np.sqrt(rr)
-        for it in range(100000):
-            v = A @ d
-            al = rr / (d @ v)
-            r -= al * v
-            rrn = r @ r
-            if np.sqrt(rrn) <= stop:
-                return it + 1
-            d = r + (rrn / rr) * d
-            rr = rrn
-        return 100000
-
-    vals = []
-    for _ in range(max(1, a.steps)):
-        t0 = time.perf_counter()
-        costs = oracle_iteration_costs(inp, sk, tau, active_h, (64, c["B"]), a.cpu_iters)
-        rhs = np.concatenate([sk[0], sk[1]], axis=1)
-        bank_it = max(seed_iters(rhs[:, j].copy()) for j in (0, 1, c["q"], c["q"] + 1))
-        short_it = []
-        for e in range(2):
-            w = np.zeros(n)
-            w[inp["cand"][e, 0]] = 1.0
-            w[inp["cand"][e, 1]] = -1.0
-            short_it.append(seed_iters(w))
-        solves = [(2 * c["q"], bank_it)] + [(c["B"], max(short_it))] * inp["k"]
-        vals.append(cpu_estimate(costs, solves))
-        sample_s = time.perf_counter() - t0
-    v = float(np.mean(vals))
-    cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-           "sample": (f"oracle multi-shift CG: {a.cpu_iters} timed iteration(s) at 64 and {c['B']} columns "
-                      f"({costs[64]:.2f} / {costs[c['B']]:.2f} s/iteration); iteration counts from seed CG on 4 "
-                      f"bank columns ({bank_it}) and 2 shortlist edges ({max(short_it)}), x {inp['k']} rounds; "
-                      f"{sample_s:.0f} s of host work per step")}
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Chung-Lu stand-in for com-DBLP shape)",
-            "config": {"workload": a.config, "n": n, "m": int(len(inp["E"])), "N": inp["N"], "K": c["K"],
-                       "q": c["q"], "B": c["B"], "k": inp["k"], "s": c["s"], "sigma": c["sigma"], "tol": c["tol"]},
-            "cpu_baseline": cpu, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    t0 = time.perf_counter()
+    parts = oracle_round_parts(inp, a.warmup + a.steps, warm=1 + a.warmup)
+    run_s = time.perf_counter() - t0
+    per, greedy_s, it_s = cpu_round_estimate(parts, rec["fp64_per_round"], max(rec["fp64_bank"]), inp["k"], c["q"])
+    cpu = {"value": per, "unit": UNIT, "cores": 1, "kind": "port", "greedy_s": greedy_s,
+           "sample": (f"oracle multi-shift CG on the shortlist solve ({c['B']} columns, {parts['p']} poles, "
+                      f"{parts['nA']} active rows): {a.steps} timed iterations of {it_s:.2f} s x "
+                      f"{np.mean(rec['fp64_per_round']):.0f} seed iterations per round (FP64 GPU counts) + scoring "
+                      f"{parts['score_s']:.2f} s + maintenance {parts['maintain_s']:.2f} s; one core")}
+    line = {"impl": "reference", "metric": METRIC, "value": per, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": it_s * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Chung-Lu stand-in for the %s shape)" % (
+                "com-LiveJournal" if a.config == "full-n4M" else a.config),
+            "config": {"workload": a.config, "n": inp["n"], "m": int(len(inp["E"])), "N": inp["N"], "K": c["K"],
+                       "q": c["q"], "B": c["B"], "k": inp["k"], "s": c["s"], "sigma": c["sigma"], "tol": c["tol"],
+                       "step": "one multi-shift CG iteration of a round's shortlist solve (value: s/round)"},
+            "greedy_s": greedy_s, "timed_run_s": run_s,
+            "cpu_baseline": cpu, "e2e": {"value": per, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
     args = parse()
-    if args.impl == "reference" and args.config in ("batch48", "full-n4M"):
-        why = {"batch48": "the many-graphs workload has no reference arm: the reference solves one graph per call",
-               "full-n4M": "the full-scale solve has no reference arm here: the oracle's FP64 NumPy solve of a "
-                           "4M-vertex graph takes hours on the host cores"}[args.config]
-        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+    if args.impl == "reference" and args.config == "batch48":
+        print(json.dumps({"impl": "reference", "unavailable": "the many-graphs workload has no reference arm: "
+                          "the reference solves one graph per call"}), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     elif args.config == "batch48":
         run_batch(args)
-    elif args.config == "full-n4M":
-        run_full(args)
+    elif args.solve:
+        run_solve(args)
     else:
-        run_ours(args)
+        run_greedy(args)

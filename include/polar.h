@@ -138,22 +138,30 @@ int polar_spmm(const polar_graph* g, int precision, int R, double shift, const v
                void* d_Y, int ldy, void* d_scratch, polar_stream_t stream);
 /* Same apply as polar_spmm with the heavy-row scratch in a fixed 8 MiB device array inside
  * the library, so the call allocates nothing.  No counterpart in the reference: it serves
- * callers that may not allocate device memory when they apply the operator.  Returns
- * POLAR_ERR_WORKSPACE when polar_spmm_scratch_bytes(g, precision, R) exceeds 8 MiB.  The
- * first call on each device resolves the array's address (cudaGetSymbolAddress) and should
- * come before any stream capture.  All calls on a device share the array: calls that
- * overlap in time race and must be serialised by the caller. */
+ * callers that may not allocate device memory when they apply the operator.  Arguments are
+ * checked as polar_spmm checks them before anything is queued (POLAR_ERR_BAD_ARG leaves
+ * the stream untouched); POLAR_ERR_WORKSPACE when polar_spmm_scratch_bytes(g, precision, R)
+ * exceeds 8 MiB.  The first call on each device, and the first call in a new context (for
+ * instance after cudaDeviceReset), resolves the array's address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  All calls on a device share the array: calls
+ * that overlap in time race and must be serialised by the caller. */
 int polar_spmm_noalloc(const polar_graph* g, int precision, int R, double shift, const void* d_X, int ldx,
                        void* d_Y, int ldy, polar_stream_t stream);
 
 /* ---- multi-shift CG (polar_gpu.py:88-133) ----
- * Solves (M + tau_j I) U_j = W for all p poles and R columns in ONE persistent
- * cooperative launch.  W: n x R FP64 row-major (ldw).  Pole iterates are kept on the nA
- * active rows (d_active: ids ascending; d_active_pos: n entries, row -> active index or
- * -1).  Outputs: X_out[p][nA][ldx] (x_f32 ? float : double) written at column offset
- * 0..R-1, h_out[p][R] (tracked ||U_j[:,c]||^2, only when track), iters_out[R].
- * maxit: iteration cap (status POLAR_ERR_ITER_CAP when hit).  The call returns after the
- * launch; polar_msolve_finish synchronises the stream and returns the solve status. */
+ * Solves (M + tau_j I) U_j = W for all p poles and R columns.  W: n x R FP64 row-major
+ * (ldw).  Pole iterates are kept on the nA active rows (d_active: ids ascending;
+ * d_active_pos: n entries, row -> active index or -1).  Outputs: X_out[p][nA][ldx]
+ * (x_f32 ? float : double) written at column offset 0..R-1, h_out[p][R] (tracked
+ * ||U_j[:,c]||^2, only when track), iters_out[R].  maxit: iteration cap (status
+ * POLAR_ERR_ITER_CAP when hit).
+ * BLOCKING with the default driver (polar_set_solver_mode(0)): the call queues blocks of
+ * 16 iterations on `stream` as CUDA-graph launches and synchronises `stream` after each
+ * block to read the convergence flags, so it returns only when the solve has ended (the
+ * host loop stands in for the reference's host-side convergence check every 8 iterations,
+ * polar_gpu.py:126).  It therefore cannot be captured into a caller's CUDA graph.  With
+ * driver 1 the call returns after one cooperative launch.  In both cases
+ * polar_msolve_finish synchronises the stream and returns the solve status. */
 size_t polar_msolve_workspace_bytes(const polar_graph* g, int precision, int R, int p, int nA);
 int polar_msolve(const polar_graph* g, int precision, const double* d_W, int ldw, int R,
                  const double* d_tau, int p, const int32_t* d_active, const int32_t* d_active_pos,
@@ -179,6 +187,12 @@ int polar_sell_rows(int precision, int R);
 void polar_set_spmm_lane_bytes(int bytes);
 /* 1 (default): polar_sell_rows reports the sliced-ELL height the solver uses; 0: CSR rows. */
 void polar_set_sell(int on);
+/* L2 eviction priorities of the solver's SpMM and direction update (default driver only):
+ * mode 0 none; 1: the first hot_bytes / (row bytes) rows of the direction (the most
+ * gathered rows of a degree-ordered graph) are gathered and stored with evict_last, the
+ * neighbour indices and the SpMM output with evict_first; 2: as 1, with gathers of the
+ * other rows evict_first too.  Caching only: results are identical in every mode. */
+int polar_set_l2_policy(int mode, size_t hot_bytes);
 
 /* ---- batched multi-shift solves (many graphs at once) ----
  * Replaces a loop of realworld/polar_gpu.py:88-133 (msolve) calls, one per graph: the

@@ -14,7 +14,7 @@ from .synth import chung_lu, candidates
 
 __version__ = "0.1.0"
 
-_DEVICE_NAMES = ("Graph", "Op", "msolve", "Counter", "polar", "true_marginals", "degree_greedy", "random_set",
+_DEVICE_NAMES = ("Graph", "Op", "msolve", "Counter", "polar", "Greedy", "true_marginals", "degree_greedy", "random_set",
                  "FracTrace", "relaxed_gradient", "relaxed_objective")
 
 
@@ -27,7 +27,7 @@ def __getattr__(name):
     if name in ("msolve", "Counter"):
         from . import solver
         return getattr(solver, name)
-    if name in ("polar", "true_marginals", "degree_greedy", "random_set"):
+    if name in ("polar", "Greedy", "true_marginals", "degree_greedy", "random_set"):
         from . import greedy
         return getattr(greedy, name)
     if name in ("FracTrace", "relaxed_gradient", "relaxed_objective"):

@@ -83,6 +83,85 @@ POLAR_D void vstore_cs(T* p, const T (&in)[V]) {
 }
 
 // ---------------------------------------------------------------------------------------
+// L2 eviction priority per access (createpolicy + .L2::cache_hint, sm_80+).  The SpMM's
+// gathers are skewed: on degree-ordered graphs a prefix of rows takes most of them, so
+// those rows are loaded (and, by the direction update, stored) with evict_last, while
+// data read or written once per pass (neighbour indices, v) goes with evict_first and
+// cannot push the prefix out of L2.  The hints change caching only, never results.
+POLAR_D uint64_t l2_policy(int kind) {  // 0 normal, 1 evict_last, 2 evict_first
+  uint64_t p;
+  if (kind == 1)
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  else if (kind == 2)
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  else
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+POLAR_D void ld_hint(float4& v, const void* p, uint64_t pol) {
+  asm volatile("ld.global.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
+}
+POLAR_D void ld_hint(float2& v, const void* p, uint64_t pol) {
+  asm volatile("ld.global.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(p), "l"(pol));
+}
+POLAR_D void ld_hint(float& v, const void* p, uint64_t pol) {
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+}
+POLAR_D void ld_hint(double2& v, const void* p, uint64_t pol) {
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+}
+POLAR_D void ld_hint(double& v, const void* p, uint64_t pol) {
+  asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+}
+POLAR_D int ld_hint_i32(const int* p, uint64_t pol) {
+  int v;
+  asm volatile("ld.global.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+POLAR_D void st_hint(void* p, const float4& v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1,%2,%3,%4}, %5;"
+               ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "l"(pol) : "memory");
+}
+POLAR_D void st_hint(void* p, const float2& v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1,%2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
+}
+POLAR_D void st_hint(void* p, const float& v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
+POLAR_D void st_hint(void* p, const double2& v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1,%2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol) : "memory");
+}
+POLAR_D void st_hint(void* p, const double& v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+
+template <typename T, int V>
+POLAR_D void vload_hint(T (&out)[V], const T* p, uint64_t pol) {
+  constexpr int VW = VecWidth<T, V>::value;
+#pragma unroll
+  for (int c = 0; c < V / VW; ++c) {
+    VecU<T, VW> u;
+    ld_hint(u.v, p + c * VW, pol);
+#pragma unroll
+    for (int i = 0; i < VW; ++i) out[c * VW + i] = u.a[i];
+  }
+}
+
+template <typename T, int V>
+POLAR_D void vstore_hint(T* p, const T (&in)[V], uint64_t pol) {
+  constexpr int VW = VecWidth<T, V>::value;
+#pragma unroll
+  for (int c = 0; c < V / VW; ++c) {
+    VecU<T, VW> u;
+#pragma unroll
+    for (int i = 0; i < VW; ++i) u.a[i] = in[c * VW + i];
+    st_hint(p + c * VW, u.v, pol);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // Programmatic dependent launch (sm_90+).  A kernel launched with programmatic stream
 // serialization may start while its predecessor is still running; pdl_wait blocks until
 // the predecessor grid has completed and its memory is visible (a no-op for an ordinary

@@ -499,6 +499,18 @@ using namespace polar;
 
 extern "C" void polar_set_barrier_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 1; }
 
+// L2 policy of the kernel-per-phase driver (SolvePrm::l2_mode / hot_rows).
+static int g_l2_mode = 0;
+static size_t g_l2_hot_bytes = size_t(64) << 20;
+
+extern "C" int polar_set_l2_policy(int mode, size_t hot_bytes) {
+  clear_error();
+  if (mode < 0 || mode > 2) return set_error(POLAR_ERR_BAD_ARG, "l2 mode must be 0, 1 or 2");
+  g_l2_mode = mode;
+  g_l2_hot_bytes = hot_bytes;
+  return POLAR_OK;
+}
+
 namespace polar {
 int mk_spmm_lanes(int precision, int ld);
 int mk_sell_rows(int precision, int ld);
@@ -591,6 +603,10 @@ static void fill_prm(SolvePrm<TT>& prm, const polar_graph* g, int R, int ld, int
   prm.dlo = sizeof(TT) == 4 ? (float*)(ws + L.off[33]) : nullptr;
   prm.nbh = 0;
   prm.timeout_ns = g_timeout_ns;
+  // the hint path lives in the kernel-per-phase kernels only
+  prm.l2_mode = composed ? g_l2_mode : 0;
+  const long long hot = (long long)(g_l2_hot_bytes / ((size_t)ld * sizeof(TT)));
+  prm.hot_rows = (int)(hot < g->n ? hot : g->n);
 }
 
 extern "C" int polar_msolve(const polar_graph* g, int precision, const double* d_W, int ldw, int R,
@@ -773,6 +789,7 @@ static int batch_graph_run(const polar_msolve_problem* probs, int nprob, int ld,
     if (e != cudaSuccess) return set_cuda_error("cudaMemsetAsync (batch)", e);
     fill_prm(prm[b], q.g, q.R, ld, q.p, q.nA, q.tol, q.maxit, q.track, q.d_W, q.ldw, q.d_tau, q.d_active,
              q.d_active_pos, q.d_X_out, q.x_f32, q.ldx, q.d_h_out, q.d_iters_out, ws, L[b], true);
+    prm[b].hot_rows /= nprob;  // concurrent solves share the L2
     // two row items per thread of the full grid count as a full share
     const double items = (double)q.g->n * (ld / VEC);
     const double f = items / ((double)full * kBlock * 2.0);

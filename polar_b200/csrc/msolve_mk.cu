@@ -210,6 +210,9 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
     for (int c = lane; c < ld; c += 32) wred[c] = 0.0;
     __syncwarp();
   }
+  const uint64_t pol_hot = l2_policy(P.l2_mode ? 1 : 0);
+  const uint64_t pol_cold = l2_policy(P.l2_mode == 2 ? 2 : 0);
+  const uint64_t pol_stream = l2_policy(P.l2_mode ? 2 : 0);
   if (MODE == 1 || MODE == 3) {
     constexpr int LB = CPL * (int)sizeof(T);
     constexpr int U = (POLAR_HEAVY_BYTES / LB) > 1 ? (POLAR_HEAVY_BYTES / LB) : 1;
@@ -233,7 +236,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
 #pragma unroll
       for (int q = 0; q < kChunkMax / 32; ++q) {
         const int k = 32 * q + lane;
-        if (k < cnt) s_idx[warp][k] = __ldg(g.d_indices + lo + k);
+        if (k < cnt) s_idx[warp][k] = ld_hint_i32(g.d_indices + lo + k, pol_stream);
       }
       __syncwarp();
       A acc[CPL];
@@ -248,7 +251,8 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
         for (int uu = 0; uu < U; ++uu)
           if (on && u0 + uu < nu) {
             const int t = grp + gpw * (u0 + uu);
-            vload<T, CPL>(xv[uu], P.d + (size_t)s_idx[warp][t] * ld + rg.col);
+            const int j = s_idx[warp][t];
+            vload_hint<T, CPL>(xv[uu], P.d + (size_t)j * ld + rg.col, row_policy(P, j, pol_hot, pol_cold));
             wv[uu] = W ? (A)__ldg(g.d_wts + lo + t) : A(1);
           }
 #pragma unroll
@@ -360,11 +364,12 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       for (int k = 0; k < w; k += U) {
         int jj[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) jj[u] = (k + u < w) ? __ldg(sp + (size_t)(k + u) * S) : -1;
+        for (int u = 0; u < U; ++u) jj[u] = (k + u < w) ? ld_hint_i32(sp + (size_t)(k + u) * S, pol_stream) : -1;
         T xv[U][CPL];
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          if (go && jj[u] >= 0) vload<T, CPL>(xv[u], P.d + (size_t)jj[u] * ld + rg.col);
+          if (go && jj[u] >= 0)
+            vload_hint<T, CPL>(xv[u], P.d + (size_t)jj[u] * ld + rg.col, row_policy(P, jj[u], pol_hot, pol_cold));
 #pragma unroll
         for (int u = 0; u < U; ++u)
           if (jj[u] >= 0) {
@@ -377,12 +382,12 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
       // y_i = (deg + sigma + added + shift) x_i - acc, formed in place in acc
       T xi[CPL];
       if (go) {
-        vload<T, CPL>(xi, P.d + (size_t)row * ld + rg.col);
+        vload_hint<T, CPL>(xi, P.d + (size_t)row * ld + rg.col, row_policy(P, row, pol_hot, pol_cold));
         const double dg = (double)deg + g.sigma + shift;
         T yv[CPL];
 #pragma unroll
         for (int v = 0; v < CPL; ++v) yv[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
-        vstore<T, CPL>(P.v + (size_t)row * ld + rg.col, yv);
+        vstore_hint<T, CPL>(P.v + (size_t)row * ld + rg.col, yv, pol_stream);
 #pragma unroll
         for (int v = 0; v < CPL; ++v) acc[v] = (A)yv[v];
       }
@@ -546,6 +551,8 @@ __global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_dir(const __grid
       any_on |= on[v];
     }
     if (any_on) {
+      const uint64_t pol_hot = l2_policy(P.l2_mode ? 1 : 0);
+      const uint64_t pol_norm = l2_policy(0);
       // FP64 r doubles the registers of a row item: fewer items in flight for wide FP32 rows
       constexpr int U = (sizeof(T) == 4 && VEC >= 4 && POLAR_STREAM_U > 2) ? 2 : POLAR_STREAM_U;
       for (long long e0 = tid; e0 < nvec; e0 += U * nth) {
@@ -566,7 +573,8 @@ __global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_dir(const __grid
 #pragma unroll
           for (int v = 0; v < VEC; ++v)
             if (on[v]) dv[u][v] = rv[u][v] + be_c[v] * dv[u][v];
-          store_dir<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col);
+          store_dir_hint<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col, row_policy(P, ii[u], pol_hot, pol_norm),
+                                 pol_norm);
         }
       }
     }

@@ -60,7 +60,18 @@ template <typename T> struct SolvePrm {
   int* ctl;  // [0]=status [1]=err [2]=where [3]=any  [4..5]=barrier count/gen
   long long* stats;  // [0]=iterations [1]=flushes [2..7]=phase ns (CTA 0 view)
   uint64_t timeout_ns;
+  // L2 policy of the kernel-per-phase driver: rows [0, hot_rows) of d are gathered and
+  // stored with evict_last; l2_mode 0: no hints, 1: cold gathers evict_normal, streamed
+  // data evict_first, 2: cold gathers evict_first as well.
+  int hot_rows;
+  int l2_mode;
 };
+
+// Policy for a gather or store of row i of d.
+template <typename T>
+POLAR_D uint64_t row_policy(const SolvePrm<T>& P, long long i, uint64_t hot, uint64_t cold) {
+  return i < P.hot_rows ? hot : cold;
+}
 
 // Direction of one row item in FP64: d (+ dlo when the remainder is kept).  store_dir
 // writes d = (T)x and, with a remainder, dlo = (float)(x - d).
@@ -89,6 +100,22 @@ POLAR_D void store_dir(const SolvePrm<T>& P, const double (&in)[VEC], size_t o) 
 #pragma unroll
     for (int v = 0; v < VEC; ++v) lo[v] = (float)(in[v] - (double)hi[v]);
     vstore<float, VEC>(P.dlo + o, lo);
+  }
+}
+
+// store_dir with L2 policies: `dpol` for the SpMM's copy d (evict_last on the gathered
+// prefix keeps it resident into the next SpMM), `lopol` for the remainder.
+template <typename T, int VEC>
+POLAR_D void store_dir_hint(const SolvePrm<T>& P, const double (&in)[VEC], size_t o, uint64_t dpol, uint64_t lopol) {
+  T hi[VEC];
+#pragma unroll
+  for (int v = 0; v < VEC; ++v) hi[v] = (T)in[v];
+  vstore_hint<T, VEC>(P.d + o, hi, dpol);
+  if (P.dlo) {
+    float lo[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) lo[v] = (float)(in[v] - (double)hi[v]);
+    vstore_hint<float, VEC>(P.dlo + o, lo, lopol);
   }
 }
 
