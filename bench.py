@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--autotune", default="auto", choices=["auto", "on", "off"],
                     help="SpMM layout tuning of the shortlist width (auto: graphs under 2M vertices)")
     ap.add_argument("--l2", default=None, help="L2 policy MODE:MB for the solver (polar_set_l2_policy)")
+    ap.add_argument("--residual", type=int, default=None, choices=[32, 64],
+                    help="residual storage of the mixed-precision solve (polar_set_mixed_residual)")
     ap.add_argument("--solve", action="store_true", help="one shortlist solve with its kernel table")
     ap.add_argument("--quick", action="store_true", help="--solve: 48-iteration solves (an ncu-sized case)")
     ap.add_argument("--cache", default=None, help="directory for generated workloads (.npz, reused when present)")
@@ -290,6 +292,8 @@ def run_greedy(a):
     if a.l2:
         mode, mb = a.l2.split(":")
         _lib.check(lib.polar_set_l2_policy(int(mode), int(float(mb) * (1 << 20))), "l2 policy")
+    if a.residual:
+        _lib.check(lib.polar_set_mixed_residual(a.residual), "residual storage")
     t_setup = time.perf_counter()
     inp = build_inputs(a)
     n, N, k, E, cand, c = inp["n"], inp["N"], inp["k"], inp["E"], inp["cand"], inp["cfg"]
@@ -703,6 +707,70 @@ def run_solve(a):
     print(json.dumps(line), flush=True)
 
 
+def run_diff(a):
+    """Differentiation workload: Chung–Lu n = 1,134,890 (~2.99M edges, exponent 2.2, seed 3),
+    sigma = 1e-2, s = 0.5, K = 24 poles; 4,096 candidate non-edges with relaxed weights
+    w ~ U[0, 1].  Times FracTrace's two halves on the device (the grouped forward f_s with
+    f_{s+1} for d f / d sigma, and the adjoint d f / d w for all 4,096 weights), checks
+    sampled adjoint entries against central differences (h = 1e-4) computed from solves
+    that do not share the adjoint's, and checks the adjoint against the dense FP64
+    eigendecomposition gradient on a 3,000-vertex induced subgraph."""
+    import torch
+
+    import polar_b200 as pg
+    from polar_b200.adjoint import relaxed_central_difference, relaxed_gradient, relaxed_objective, relaxed_rule
+    from oracle import polar_oracle as O
+    from polar_b200.synth import candidates
+    torch.cuda.set_device(0)
+    inp = build_inputs(a)
+    n, E, cand, c = inp["n"], inp["E"], inp["cand"], inp["cfg"]
+    rng = np.random.default_rng(c["seed"])
+    w = rng.uniform(0.0, 1.0, len(cand))
+    G = pg.Graph(n, E, c["sigma"])
+    tau, om = relaxed_rule(G, c["s"], K=c["K"])
+    tol = c["tol"]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
+    out = {}
+    for prec in ("fp64", "mixed"):
+        grad, tg = timed(lambda: relaxed_gradient(G, cand, w, c["s"], tau=tau, om=om, tol=tol, precision=prec))
+        out[prec] = {"gradient_s": tg, "grad": grad}
+    (f, f_next), tf = timed(lambda: relaxed_objective(G, cand, w, c["s"], tau=tau, om=om, tol=tol, with_next=True))
+    g64 = out["fp64"]["grad"]
+    sample = [int(i) for i in rng.choice(np.flatnonzero(w >= 1e-3), 8, replace=False)]
+    fd = []
+    for i in sample:
+        v, t = timed(lambda: relaxed_central_difference(G, cand, w, c["s"], i, 1e-4, tau=tau, om=om, tol=tol))
+        fd.append({"i": i, "fd": v, "grad": float(g64[i]), "rel_err": abs(v - g64[i]) / abs(v), "seconds": t})
+    # dense check: induced subgraph on the 3,000 lowest ids (the hubs and their mutual edges)
+    ns = 3000
+    Es = E[(E[:, 0] < ns) & (E[:, 1] < ns)]
+    cs = candidates(ns, Es, 256, c["seed"] + 11)
+    ws = rng.uniform(0.0, 1.0, len(cs))
+    Gs = pg.Graph(ns, Es, c["sigma"])
+    ts, oms = relaxed_rule(Gs, c["s"], K=c["K"])
+    gs = relaxed_gradient(Gs, cs, ws, c["s"], tau=ts, om=oms, tol=1e-12)
+    d = O.relaxed_dense(ns, Es, c["sigma"], cs, ws, c["s"], ts, oms)
+    line = {"metric": "relaxed-weight objective and adjoint (FracTrace halves)", "unit": "s",
+            "value": out["fp64"]["gradient_s"], "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": a.config, "n": n, "m": int(len(E)), "candidates": len(cand), "K": c["K"],
+                       "s": c["s"], "sigma": c["sigma"], "tol": tol},
+            "forward_s": tf, "f": f, "dsigma": -c["s"] * f_next,
+            "gradient_fp64_s": out["fp64"]["gradient_s"], "gradient_mixed_s": out["mixed"]["gradient_s"],
+            "mixed_vs_fp64_max_rel": float(np.max(np.abs(out["mixed"]["grad"] - g64) / np.abs(g64))),
+            "central_differences": fd, "max_rel_err_vs_central_differences": max(x["rel_err"] for x in fd),
+            "dense_subgraph": {"n": ns, "m": int(len(Es)), "candidates": len(cs),
+                               "max_rel_err_vs_rule": float(np.max(np.abs(gs - d["grad_q"]) / np.abs(d["grad_q"]))),
+                               "max_rel_err_vs_exact": float(np.max(np.abs(gs - d["grad"]) / np.abs(d["grad"])))}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(a):
     """The reference's algorithm on the host cores for the same workload and metric: the
     oracle (a NumPy FP64 restatement of realworld/polar_gpu.py, pinned to the reference's
@@ -746,13 +814,16 @@ def run_reference(a):
 
 if __name__ == "__main__":
     args = parse()
-    if args.impl == "reference" and args.config == "batch48":
-        print(json.dumps({"impl": "reference", "unavailable": "the many-graphs workload has no reference arm: "
-                          "the reference solves one graph per call"}), flush=True)
+    if args.impl == "reference" and args.config in ("batch48", "diff-n1.13M"):
+        print(json.dumps({"impl": "reference", "unavailable": {
+            "batch48": "the many-graphs workload has no reference arm: the reference solves one graph per call",
+            "diff-n1.13M": "the reference has no relaxed-weight objective or adjoint"}[args.config]}), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     elif args.config == "batch48":
         run_batch(args)
+    elif args.config == "diff-n1.13M":
+        run_diff(args)
     elif args.solve:
         run_solve(args)
     else:

@@ -193,6 +193,10 @@ void polar_set_sell(int on);
  * neighbour indices and the SpMM output with evict_first; 2: as 1, with gathers of the
  * other rows evict_first too.  Caching only: results are identical in every mode. */
 int polar_set_l2_policy(int mode, size_t hot_bytes);
+/* Residual storage of the mixed-precision solve (default driver): 64 (default) keeps r in
+ * FP64; 32 stores r in FP32 (rounded after every update, norms taken of the stored value),
+ * with the direction still held to FP64 accuracy as an FP32 value plus FP32 remainder. */
+int polar_set_mixed_residual(int bits);
 
 /* ---- batched multi-shift solves (many graphs at once) ----
  * Replaces a loop of realworld/polar_gpu.py:88-133 (msolve) calls, one per graph: the
@@ -265,6 +269,8 @@ int polar_pair_norms(const void* d_X, int x_f32, int p, int nA, int ldx, int col
 /* ---- proxy score + stable top-B (polar_gpu.py:208-211, 219-221) ----
  * score[e] = sum_j om_j h_je / (1 + t_je + (sigma + tau_j) h_je)   (obj 0, 'frac'/'er')
  *          = log1p(t_0e + sigma h_0e)                                (obj 1, 'logdet')
+ *          = sum_j om_j h_je                                         (obj 2: the sketched
+ *            adjoint d f_s / d w_e at w = 0, the candidate screen; no reference counterpart)
  * Dead candidates (live[e] == 0) score -inf.  The B best by (score desc, index asc) —
  * the order of a stable argsort of -score — go to out_idx / out_score (device).
  * d_tmp: polar_topb_tmp_bytes(N, B) bytes. */

@@ -26,6 +26,7 @@ SCHEMES = {
     "v32": dict(v=True),
     "r64": dict(d=True, dm=True, v=True, xp=True),
     "device": dict(dm=True, v=True, xp=True),
+    "device_r32": dict(r=True, dm=True, v=True, xp=True),
 }
 
 

@@ -99,6 +99,7 @@ SIGNATURES = {
     "polar_set_spmm_lane_bytes": (None, [_I]),
     "polar_set_sell": (None, [_I]),
     "polar_set_l2_policy": (_I, [_I, _S]),
+    "polar_set_mixed_residual": (_I, [_I]),
     "polar_msolve_batch_workspace_bytes": (_S, [_GP, _I, _I, _I, _I]),
     "polar_msolve_batch": (_I, [ctypes.POINTER(MsolveProblem), _I, _I, _P]),
     "polar_block_orth": (_I, [_P, _I64, _I, _P, _P, _I, _P]),

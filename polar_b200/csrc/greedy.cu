@@ -114,6 +114,10 @@ __global__ void __launch_bounds__(kTopBlock) score_block_topb_kernel(const doubl
     if (e < N) {
       if (obj == 1) {
         v = log1p(t[e] + sigma * h[e]);
+      } else if (obj == 2) {
+        double acc = 0.0;
+        for (int j = 0; j < p; ++j) acc += om[j] * h[(size_t)j * N + e];
+        v = acc;
       } else {
         double acc = 0.0;
         for (int j = 0; j < p; ++j) {
@@ -436,6 +440,7 @@ extern "C" int polar_score_topb(const double* d_h, const double* d_t, const doub
   if (!d_h || !d_t || !d_tau || !d_om || !d_live || !d_out_idx || !d_tmp || p < 1 || N < 1)
     return set_error(POLAR_ERR_BAD_ARG, "bad arguments");
   if (B < 1 || B > kMaxB || B > N) return set_error(POLAR_ERR_BAD_ARG, "B out of range");
+  if (obj < 0 || obj > 2) return set_error(POLAR_ERR_BAD_ARG, "obj must be 0, 1 or 2");
   const long long per = (long long)kTopBlock * kTopPer;
   const int nb = (int)((N + per - 1) / per);
   cudaStream_t st = (cudaStream_t)stream;

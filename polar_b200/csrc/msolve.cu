@@ -499,6 +499,16 @@ using namespace polar;
 
 extern "C" void polar_set_barrier_timeout_ns(uint64_t ns) { g_timeout_ns = ns ? ns : 1; }
 
+// Residual storage of the mixed-precision kernel-per-phase driver: 64 (FP64) or 32.
+static int g_mixed_residual_bits = 64;
+
+extern "C" int polar_set_mixed_residual(int bits) {
+  clear_error();
+  if (bits != 32 && bits != 64) return set_error(POLAR_ERR_BAD_ARG, "residual bits must be 32 or 64");
+  g_mixed_residual_bits = bits;
+  return POLAR_OK;
+}
+
 // L2 policy of the kernel-per-phase driver (SolvePrm::l2_mode / hot_rows).
 static int g_l2_mode = 0;
 static size_t g_l2_hot_bytes = size_t(64) << 20;
@@ -569,6 +579,8 @@ static void fill_prm(SolvePrm<TT>& prm, const polar_graph* g, int R, int ld, int
   prm.h_out = d_h_out;
   prm.iters_out = (long long*)d_iters_out;
   prm.r = (double*)(ws + L.off[0]);
+  // the FP32 residual (when chosen) takes the first half of the FP64 residual's region
+  prm.r32 = (composed && sizeof(TT) == 4 && g_mixed_residual_bits == 32) ? (float*)(ws + L.off[0]) : nullptr;
   prm.d = (TT*)(ws + L.off[1]);
   prm.v = (TT*)(ws + L.off[2]);
   prm.hist = (TT*)(ws + L.off[3]);

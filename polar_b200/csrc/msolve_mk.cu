@@ -80,9 +80,10 @@ __global__ void __launch_bounds__(kBlock) mk_init(const __grid_constant__ SolveP
     for (int v = 0; v < VEC; ++v) {
       const int c = rg.col + v;
       wd[v] = (c < P.R) ? __ldg(P.W + (size_t)i * P.ldw + c) : 0.0;
-      acc[v] += wd[v] * wd[v];
     }
-    vstore<double, VEC>(P.r + (size_t)i * ld + rg.col, wd);
+    store_res<T, VEC>(P, wd, (size_t)i * ld + rg.col);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] += wd[v] * wd[v];
     store_dir<T, VEC>(P, wd, (size_t)i * ld + rg.col);
   }
   reduce_cols_to_part<VEC>(acc, rg.G, ld, red, P.part + (size_t)blockIdx.x * ld);
@@ -484,7 +485,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_resid(const __gr
         const long long e = e0 + u * nth;
         ii[u] = e < nvec ? (e >> lgG) : -1;
         if (ii[u] >= 0) {
-          vload<double, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+          load_res<T, VEC>(P, rv[u], (size_t)ii[u] * ld + rg.col);
           vload<T, VEC>(vv[u], P.v + (size_t)ii[u] * ld + rg.col);
           ai[u] = __ldg(P.active_pos + ii[u]);
         }
@@ -494,12 +495,14 @@ __global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_resid(const __gr
         if (ii[u] < 0) continue;
         T rt[VEC];
 #pragma unroll
-        for (int v = 0; v < VEC; ++v) {
+        for (int v = 0; v < VEC; ++v)
           if (on[v]) rv[u][v] = rv[u][v] - a_c[v] * (double)vv[u][v];
+        store_res<T, VEC>(P, rv[u], (size_t)ii[u] * ld + rg.col);
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) {
           racc[v] += rv[u][v] * rv[u][v];
           rt[v] = (T)rv[u][v];
         }
-        vstore<double, VEC>(P.r + (size_t)ii[u] * ld + rg.col, rv[u]);
         if (ai[u] >= 0) vstore_cs<T, VEC>(hslot + (size_t)ai[u] * ld + rg.col, rt);
       }
     }
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_dir(const __grid
           const long long e = e0 + u * nth;
           ii[u] = e < nvec ? (e >> lgG) : -1;
           if (ii[u] >= 0) {
-            vload<double, VEC>(rv[u], P.r + (size_t)ii[u] * ld + rg.col);
+            load_res<T, VEC>(P, rv[u], (size_t)ii[u] * ld + rg.col);
             load_dir<T, VEC>(P, dv[u], (size_t)ii[u] * ld + rg.col);
           }
         }
@@ -846,9 +849,10 @@ struct MkSolver {
     const double s = sizeof(T), n = P.n, R = P.R, nA = P.nA;
     // algorithmic bytes per launch (unweighted CSR: values implicit, diagonal from indptr)
     const double b_spmm = 4.0 * (n + 1) + 4.0 * P.g.nnz + 2.0 * s * n * R;
-    // r is FP64 in both precisions; mixed precision keeps the direction's FP32 remainder
-    const double b_resid = (16.0 + s) * n * R + s * nA * R;
-    const double b_dir = 24.0 * n * R;  // r (8) + direction (8) in, direction (8) out
+    // r is FP64, or FP32 with r32; mixed precision keeps the direction's FP32 remainder
+    const double rb = P.r32 ? 4.0 : 8.0;
+    const double b_resid = (2.0 * rb + s) * n * R + s * nA * R;
+    const double b_dir = (rb + 16.0) * n * R;  // r + direction (8) in, direction (8) out
     b_flush = (4.0 * P.p + kHist) * s * nA * R;
     const int g0 = scaled(occ_grid(mk_init<T, VEC>, kBlock), f, 1);
     const int cpl = spmm_cpl<T>(P.ld, VEC);

@@ -44,6 +44,7 @@ template <typename T> struct SolvePrm {
   // reads both; dlo == nullptr: d is the direction itself.  v, the history and the
   // shifted iterates are T.
   double* r;
+  float* r32;  // mixed precision with a rounded residual: r in FP32 here (r unused); else null
   float* dlo;
   T *d, *v, *hist, *Pb, *Xb;
   typename AccOf<T>::type* chunk_part;
@@ -71,6 +72,36 @@ template <typename T> struct SolvePrm {
 template <typename T>
 POLAR_D uint64_t row_policy(const SolvePrm<T>& P, long long i, uint64_t hot, uint64_t cold) {
   return i < P.hot_rows ? hot : cold;
+}
+
+// Residual of one row item: the FP64 r, or the FP32 residual when r32 is set.
+template <typename T, int VEC>
+POLAR_D void load_res(const SolvePrm<T>& P, double (&out)[VEC], size_t o) {
+  if (P.r32) {
+    float t[VEC];
+    vload<float, VEC>(t, P.r32 + o);
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) out[v] = (double)t[v];
+  } else {
+    vload<double, VEC>(out, P.r + o);
+  }
+}
+
+// Stores a residual row item; with r32 it is rounded first and `x` receives the stored
+// value, so that norms and recurrences use the residual as stored.
+template <typename T, int VEC>
+POLAR_D void store_res(const SolvePrm<T>& P, double (&x)[VEC], size_t o) {
+  if (P.r32) {
+    float t[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) {
+      t[v] = (float)x[v];
+      x[v] = (double)t[v];
+    }
+    vstore<float, VEC>(P.r32 + o, t);
+  } else {
+    vstore<double, VEC>(P.r + o, x);
+  }
 }
 
 // Direction of one row item in FP64: d (+ dlo when the remainder is kept).  store_dir

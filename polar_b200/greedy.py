@@ -84,6 +84,7 @@ class Greedy:
         self.obj, self.naive, self.B, self.tol, self.maxit, self.trace = obj, naive, B, tol, maxit, trace
         tau, om, _ = poles(obj, s, G.sigma, G.Lam(k), eps, K=K)
         p = self.p = len(tau)
+        self.s = s
         if sketch is None:
             sketch = sketches(G, cand, q, seed, kind)
         Z, F, Gc = sketch
@@ -152,6 +153,39 @@ class Greedy:
             _lib.check(lib.polar_pair_norms(self.XY.data_ptr(), self.x_f32, p, nA, 2 * q, col, q, self.ea_d.data_ptr(),
                                             self.eb_d.data_ptr(), N, dst.data_ptr(), self.stream), "pair_norms")
         self.banked = True
+
+    def screen(self, M, exact=False):
+        """Keep live only the M candidates with the largest adjoint gradient of the relaxed
+        objective at w = 0, d f_s / d w_e = sum_j om_j ||(A + tau_j)^{-1} b_e||^2 (the
+        quantity the proxy's numerator sketches), before any proxy or shortlist; ties go to
+        the lower index.  exact=False reads it from the bank's caches (sum_j om_j h_je, one
+        pass over p x N); exact=True solves for every candidate's b_e (N / 64 multi-shift
+        solves, for pools up to ~10^5).  Runs after bank()."""
+        if not self.banked:
+            self.bank()
+        M = int(M)
+        if M >= int(self.live_h.sum()):
+            return
+        if exact:
+            from .adjoint import relaxed_gradient
+            g = relaxed_gradient(self.G, self.cand, np.zeros(self.N), self.s, tau=self.tau_d.cpu().numpy(),
+                                 om=self.om_d.cpu().numpy(), tol=self.tol,
+                                 precision="mixed" if self.prec == _lib.POLAR_MIXED else "fp64")
+        else:
+            buf = torch.empty(self.N, dtype=torch.float64, device=self.dev)
+            _lib.check(self.lib.polar_score_topb(self.h.data_ptr(), self.t.data_ptr(), self.tau_d.data_ptr(),
+                                                 self.om_d.data_ptr(), self.G.sigma, self.p, self.N,
+                                                 self.live_d.data_ptr(), 2, 1, self.short_d.data_ptr(),
+                                                 self.sscore_d.data_ptr(), buf.data_ptr(), self.topb_tmp.data_ptr(),
+                                                 self.stream), "screen scores")
+            g = buf.cpu().numpy()
+        g = np.where(self.live_h, g, -np.inf)
+        keep = np.argsort(-g, kind="stable")[:M]
+        mask = np.zeros(self.N, bool)
+        mask[keep] = True
+        self.live_h &= mask
+        self.live_d.copy_(torch.as_tensor(self.live_h.astype(np.uint8)))
+        self.screened = keep
 
     def step(self, record=False):
         """One round (polar_gpu.py:215-251): proxy + stable top-B, the B-column shortlist
@@ -238,13 +272,19 @@ class Greedy:
 
 def polar(G, cand, k, s, q=128, B=16, eps=1e-2, tol=1e-7, obj="frac", sketch=None, naive=False, seed=2026,
           kind="block", trace=None, time_limit=None, *, K=None, precision="fp64", width=None, maxit=100000,
-          phases=False):
+          phases=False, screen=None, screen_exact=False):
     """Greedy POLAR (realworld/polar_gpu.py:180-254).  Returns the reference keys
     (sequence, seconds, spmv, rhs, p, rounds, truncated) plus `marginals`: the re-rank value
-    G_q(e*) of each round's winner (naive rounds: the proxy value), and `precision`."""
+    G_q(e*) of each round's winner (naive rounds: the proxy value), and `precision`.
+    screen=M: after the bank, only the M candidates with the largest adjoint gradient
+    d f_s / d w_e stay in the pool (Greedy.screen); None keeps the reference's path."""
     g = Greedy(G, cand, k, s, q=q, B=B, eps=eps, tol=tol, obj=obj, sketch=sketch, naive=naive, seed=seed, kind=kind,
                trace=trace, K=K, precision=precision, width=width, maxit=maxit, phases=phases)
     g.bank()
+    if screen is not None:
+        if obj != "frac" or naive:
+            raise ValueError("the gradient screen applies to obj='frac' without naive re-banking")
+        g.screen(screen, exact=screen_exact)
     for rnd in range(g.k):
         if rnd and time_limit is not None and time.perf_counter() - g.t0 > time_limit:
             break

@@ -109,3 +109,76 @@ def test_frac_trace_autograd():
     assert abs(float(sig.grad) - d["dsigma"]) / abs(d["dsigma"]) < 2e-3
     g = relaxed_gradient(G, cand, w, S, tau=tau, om=om, dsigma=0.5 * SIGMA, tol=1e-11)
     assert np.allclose(wt.grad.numpy(), g, rtol=1e-12)
+
+
+@pytest.mark.gpu
+def test_grouped_objective_matches_chain_and_dense():
+    """Woodbury groups (4 edges per solve, and the default column-limit group) give the
+    rank-one chain's f and f_{s+1}; both match the dense rule."""
+    import polar_b200 as pg
+    from polar_b200.adjoint import relaxed_objective
+    E, cand, w = _problem(m=10, seed=4)
+    w[3] = 0.0  # a zero weight is skipped by every form
+    tau, om = _rule(E, w.sum())
+    d = O.relaxed_dense(N, E, SIGMA, cand, w, S, tau, om)
+    G = pg.Graph(N, E, SIGMA)
+    chain = relaxed_objective(G, cand, w, S, tau=tau, om=om, tol=1e-12, with_next=True, group=1)
+    for grp in (4, None):
+        f, fn = relaxed_objective(G, cand, w, S, tau=tau, om=om, tol=1e-12, with_next=True, group=grp)
+        assert f == pytest.approx(chain[0], rel=1e-9)
+        assert fn == pytest.approx(chain[1], rel=1e-9)
+    assert chain[0] == pytest.approx(d["f_q"], rel=1e-8)
+
+
+@pytest.mark.gpu
+def test_central_difference_matches_gradient():
+    """relaxed_central_difference (a solve on the operator without edge i) against the
+    gradient (one solve on the full relaxed operator) and the dense rule, h = 1e-4."""
+    import polar_b200 as pg
+    from polar_b200.adjoint import relaxed_central_difference, relaxed_gradient
+    E, cand, w = _problem(m=12, seed=5)
+    w = np.maximum(w, 1e-3)
+    tau, om = _rule(E, w.sum())
+    d = O.relaxed_dense(N, E, SIGMA, cand, w, S, tau, om)
+    G = pg.Graph(N, E, SIGMA)
+    g = relaxed_gradient(G, cand, w, S, tau=tau, om=om, tol=1e-12)
+    for i in (0, 5, 11):
+        fd = relaxed_central_difference(G, cand, w, S, i, 1e-4, tau=tau, om=om, tol=1e-12)
+        assert fd == pytest.approx(g[i], rel=1e-5)
+        assert fd == pytest.approx(d["grad_q"][i], rel=1e-5)
+
+
+@pytest.mark.gpu
+def test_gradient_screen():
+    """polar(..., screen=M): the live pool after the bank is the top M by the sketched
+    adjoint sum_j om_j h_je (stable order), the exact screen ranks by the dense FP64
+    gradient of the rule, and a screen that holds every winner leaves the sequence alone."""
+    import torch
+    import polar_b200 as pg
+    from polar_b200.synth import candidates
+    E = chung_lu(N, 6.0, 2.5, 3, min_degree=1)
+    cand = candidates(N, E, 3000, 17)
+    G = pg.Graph(N, E, SIGMA)
+    sk = pg.sketches(G, cand, 16, 2026)
+    kw = dict(q=16, B=4, tol=1e-9, sketch=sk, K=12)
+    ref = pg.polar(G, cand, 5, S, **kw)
+    g = pg.Greedy(G, cand, 5, S, **kw)
+    g.bank()
+    score = (g.om_d[:, None] * g.h).sum(0).cpu().numpy()
+    g.screen(400)
+    want = np.sort(np.argsort(-score, kind="stable")[:400])
+    np.testing.assert_array_equal(np.flatnonzero(g.live_h), want)
+    assert np.array_equal(g.live_d.cpu().numpy().astype(bool), g.live_h)
+    rank = np.empty(len(cand), int)
+    rank[np.argsort(-score, kind="stable")] = np.arange(len(cand))
+    M = int(rank[ref["sequence"]].max()) + 1
+    res = pg.polar(G, cand, 5, S, screen=M, **kw)
+    assert res["sequence"] == ref["sequence"]
+    # exact screen: d f/d w_e at w = 0 for every candidate, against the dense rule
+    sub = cand[:300]
+    ge = pg.Greedy(G, sub, 3, S, q=16, B=4, tol=1e-11, sketch=pg.sketches(G, sub, 16, 2026), K=12)
+    ge.bank()
+    ge.screen(50, exact=True)
+    tau, om = ge.tau_d.cpu().numpy(), ge.om_d.cpu().numpy()
+    d = O.relaxed_dense(N, E, SIGMA, sub, np.zeros(len(sub)), S, tau, om)
+    np.testing.assert_array_equal(np.flatnonzero(ge.live_h), np.sort(np.argsort(-d["grad_q"], kind="stable")[:50]))
