@@ -20,6 +20,8 @@
 
 namespace polar {
 
+constexpr int kChunkMax = 256;  // neighbours per heavy-row chunk (the graph partition's CHUNK)
+
 template <typename T> struct AccOf;
 template <> struct AccOf<float> { using type = float; };
 template <> struct AccOf<double> { using type = double; };
@@ -124,10 +126,10 @@ POLAR_D void gather_rows(const polar_graph& g, const RowGroup& rg, int lo, int h
 }
 
 // Added-edge contribution for row i: acc += sum w x_k, returns sum w (to add to diag).
-template <typename T, int VEC>
+template <typename T, int VEC, typename AA = typename AccOf<T>::type>
 POLAR_D double added_terms(const polar_graph& g, const RowGroup& rg, int i, const T* X, int ld,
-                           typename AccOf<T>::type (&acc)[VEC], bool on = true) {
-  using A = typename AccOf<T>::type;
+                           AA (&acc)[VEC], bool on = true) {
+  using A = AA;
   if (g.nx == 0 || !on) return 0.0;
   const uint32_t bits = __ldg(g.d_xbits + (i >> 5));
   if (!((bits >> (i & 31)) & 1u)) return 0.0;
@@ -163,7 +165,7 @@ POLAR_D void finish_row_pre(const polar_graph& g, const RowGroup& rg, int i, int
     return;
   }
   double wadd = 0.0;
-  if constexpr (ADD) wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
+  if constexpr (ADD) wadd = added_terms<T, VEC, AA>(g, rg, i, X, ld, acc);
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
 #pragma unroll
   for (int v = 0; v < VEC; ++v) yi[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
@@ -182,7 +184,7 @@ POLAR_D void finish_row(const polar_graph& g, const RowGroup& rg, int i, int deg
     return;
   }
   double wadd = 0.0;
-  if constexpr (ADD) wadd = added_terms<T, VEC>(g, rg, i, X, ld, acc);
+  if constexpr (ADD) wadd = added_terms<T, VEC, AA>(g, rg, i, X, ld, acc);
   const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + wadd + shift;
   vload<T, VEC>(xi, X + (size_t)i * ld + rg.col);
 #pragma unroll

@@ -10,6 +10,11 @@ namespace polar {
 // heavy-row arrival counters inside the scratch; shared with polar_spmm_noalloc.
 int spmm_check_args(const polar_graph* g, int precision, int R, const void* d_X, int ldx, const void* d_Y, int ldy);
 size_t spmm_counter_offset(const polar_graph* g, int precision);
+// The L2 policy set by polar_set_l2_policy (also applied by the standalone apply) and the
+// solver's SpMM lanes per row for a padded width.
+int l2_mode_setting();
+size_t l2_hot_bytes_setting();
+int mk_spmm_lanes(int precision, int ld);
 
 int set_error(int code, const char* msg);
 int set_cuda_error(const char* what, cudaError_t e);

@@ -513,6 +513,11 @@ extern "C" int polar_set_mixed_residual(int bits) {
 static int g_l2_mode = 0;
 static size_t g_l2_hot_bytes = size_t(64) << 20;
 
+namespace polar {
+int l2_mode_setting() { return g_l2_mode; }
+size_t l2_hot_bytes_setting() { return g_l2_hot_bytes; }
+}  // namespace polar
+
 extern "C" int polar_set_l2_policy(int mode, size_t hot_bytes) {
   clear_error();
   if (mode < 0 || mode > 2) return set_error(POLAR_ERR_BAD_ARG, "l2 mode must be 0, 1 or 2");

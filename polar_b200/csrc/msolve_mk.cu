@@ -28,6 +28,7 @@
 #include "graph_ops.cuh"
 #include "host_util.h"
 #include "msolve_mk.h"
+#include "sell_spmm.cuh"
 #include "solver_core.cuh"
 
 namespace polar {
@@ -166,12 +167,6 @@ POLAR_D void apply_added_edges(const SolvePrm<T>& P, double* tmp, double* s_col)
 template <typename T> struct SpmmAcc { using type = double; };
 template <> struct SpmmAcc<float> { using type = std::conditional<POLAR_SPMM_ACC64 != 0, double, float>::type; };
 
-#ifndef POLAR_HEAVY_BYTES
-#define POLAR_HEAVY_BYTES 64
-#endif
-#ifndef POLAR_SELL_BYTES
-#define POLAR_SELL_BYTES 64
-#endif
 // CPL: columns per lane (several 16-byte accesses when wider); row group = ld / CPL lanes.
 // MODE 1: heavy chunks only (partials of d.v to part_h, no reduction); MODE 2: light rows
 // by row groups (after a MODE 1 launch); MODE 3 (unweighted graphs with a sliced-ELL copy):
@@ -199,118 +194,45 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
   bool on = false;
 #pragma unroll
   for (int v = 0; v < CPL; ++v) on |= P.act[rg.col + v] != 0;
-  // heavy rows, in chunks of at most kChunkMax neighbours, one warp per chunk.  The warp
-  // stages the chunk's indices in shared memory with one coalesced pass; row group grp
-  // then takes neighbours grp, grp + gpw, ... in batches of U independent gathers, and the
-  // groups combine by shuffles in a fixed pattern.  A row held in one chunk is finished by
-  // the warp; longer rows leave per-chunk partials that the last chunk to arrive sums in
-  // chunk order, so neither v nor d.v depends on scheduling.
-  // MODE 3 accumulates d.v in the warp's row of `red` (heavy chunks first, then slices)
+  // heavy chunks then light-row slices (sell_spmm.cuh); MODE 3 accumulates d.v in the
+  // warp's row of `red` (heavy chunks first, then slices)
   double* wred = red + warp * ld;
   if (MODE == 3) {
     for (int c = lane; c < ld; c += 32) wred[c] = 0.0;
     __syncwarp();
   }
-  const uint64_t pol_hot = l2_policy(P.l2_mode ? 1 : 0);
-  const uint64_t pol_cold = l2_policy(P.l2_mode == 2 ? 2 : 0);
-  const uint64_t pol_stream = l2_policy(P.l2_mode ? 2 : 0);
+  const GatherHints hp = make_gather_hints(P.l2_mode, P.hot_rows);
+  const int wid = blockIdx.x * kWarps + warp;
+  const int nw = gridDim.x * kWarps;
   if (MODE == 1 || MODE == 3) {
-    constexpr int LB = CPL * (int)sizeof(T);
-    constexpr int U = (POLAR_HEAVY_BYTES / LB) > 1 ? (POLAR_HEAVY_BYTES / LB) : 1;
     __shared__ int s_idx[kWarps][kChunkMax];
     double dacc[CPL];
 #pragma unroll
     for (int v = 0; v < CPL; ++v) dacc[v] = 0.0;
-    const int wid = blockIdx.x * kWarps + warp;
-    const int nw = gridDim.x * kWarps;
-    const int grp = lane / rg.G;
-    for (int ch = wid; ch < g.nchunks; ch += nw) {
-      const int h = __ldg(g.d_chunk_row + ch);
-      const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
-      const int i = __ldg(g.d_hrow + h);
-      const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
-      const bool single = (c1 - c0) == 1;
-      T xi[CPL];
-      if (on && grp == 0) vload<T, CPL>(xi, P.d + (size_t)i * ld + rg.col);
-      const int cnt = hi - lo;
-      __syncwarp();
-#pragma unroll
-      for (int q = 0; q < kChunkMax / 32; ++q) {
-        const int k = 32 * q + lane;
-        if (k < cnt) s_idx[warp][k] = ld_hint_i32(g.d_indices + lo + k, pol_stream);
-      }
-      __syncwarp();
-      A acc[CPL];
-#pragma unroll
-      for (int v = 0; v < CPL; ++v) acc[v] = A(0);
-      const int nu = cnt > grp ? (cnt - grp + gpw - 1) / gpw : 0;
-      const int numax = (cnt + gpw - 1) / gpw;
-      for (int u0 = 0; u0 < numax; u0 += U) {
-        T xv[U][CPL];
-        A wv[U];
-#pragma unroll
-        for (int uu = 0; uu < U; ++uu)
-          if (on && u0 + uu < nu) {
-            const int t = grp + gpw * (u0 + uu);
-            const int j = s_idx[warp][t];
-            vload_hint<T, CPL>(xv[uu], P.d + (size_t)j * ld + rg.col, row_policy(P, j, pol_hot, pol_cold));
-            wv[uu] = W ? (A)__ldg(g.d_wts + lo + t) : A(1);
-          }
-#pragma unroll
-        for (int uu = 0; uu < U; ++uu)
-          if (on && u0 + uu < nu) {
-#pragma unroll
-            for (int v = 0; v < CPL; ++v) acc[v] = W ? fma(wv[uu], (A)xv[uu][v], acc[v]) : acc[v] + (A)xv[uu][v];
-          }
-      }
-      for (int o = rg.G; o < 32; o <<= 1)
-#pragma unroll
-        for (int v = 0; v < CPL; ++v) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
-      if (single) {
-        if (grp == 0) {
+    heavy_chunk_pass<T, CPL, W, A>(
+        g, rg, wid, nw, P.d, ld, ld, on, s_idx[warp], chunk_part, P.hcount, hp,
+        [&](int i, int cnt, auto& acc, auto& xi) {
           T yi[CPL];
           finish_row_pre<T, CPL, false, A>(g, rg, i, cnt, shift, P.d, ld, acc, P.v, ld, xi, yi, on);
           if (on)
 #pragma unroll
             for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (double)yi[v];
-        }
-        continue;
-      }
-      if (on && grp == 0) {
-        vstore<A, CPL>(chunk_part + (size_t)ch * ld + rg.col, acc);
+        },
+        [&](int i, bool first, auto& acc, auto& xi) {
+          // each chunk adds its share of d_i . v_i; the first also the diagonal term
 #pragma unroll
-        for (int v = 0; v < CPL; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
-        if (ch == c0) {
-          const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-          const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + shift;
+          for (int v = 0; v < CPL; ++v) dacc[v] -= (double)xi[v] * (double)acc[v];
+          if (first) {
+            const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+            const double dg = (g.d_diag ? __ldg(g.d_diag + i) : (double)deg + g.sigma) + shift;
 #pragma unroll
-          for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v]);
-        }
-      }
-      __threadfence();
-      __syncwarp();
-      int old = 0;
-      if (lane == 0) old = atomicAdd(P.hcount + h, 1);
-      old = __shfl_sync(0xffffffffu, old, 0);
-      if (old == c1 - c0 - 1 && grp == 0) {
-        __threadfence();
-        A sum[CPL];
-#pragma unroll
-        for (int v = 0; v < CPL; ++v) sum[v] = A(0);
-        if (on)
-          for (int c2 = c0; c2 < c1; ++c2) {
-            A pv[CPL];
-            vload_cg<A, CPL>(pv, chunk_part + (size_t)c2 * ld + rg.col);
-#pragma unroll
-            for (int v = 0; v < CPL; ++v) sum[v] += pv[v];
+            for (int v = 0; v < CPL; ++v) dacc[v] += (double)xi[v] * (dg * (double)xi[v]);
           }
-        const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
-        T xf[CPL], yi[CPL];
-        finish_row<T, CPL, false, A>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
-        if (lane == 0) P.hcount[h] = 0;
-      }
-      __syncwarp();
-    }
+        },
+        [&](int i, int deg, auto& sum) {
+          T xf[CPL], yi[CPL];
+          finish_row<T, CPL, false, A>(g, rg, i, deg, shift, P.d, ld, sum, P.v, ld, xf, yi, on);
+        });
     if (MODE == 1) {
       // heavy-only launch: partial d.v per CTA, reduced by the light launch's last CTA
       reduce_cols_to_part<CPL>(dacc, rg.G, ld, red, P.part_h + (size_t)blockIdx.x * ld);
@@ -326,69 +248,20 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
     __syncwarp();
   }
   if (MODE == 3) {
-    // light rows in sliced ELL: a warp takes a slice of gpw degree-sorted rows and reads
-    // neighbour k of all its rows with one coalesced load.  Neighbours go in batches of U
-    // predicated gathers (short rows issue all theirs at once), the next slice's
-    // descriptors are fetched while this one is gathered, and a row's degree is the count
-    // of its valid entries (the slice holds exactly the CSR neighbours).  The row's own
-    // entries are read after its gathers.  d.v leaves the registers: after each slice the
-    // products x_i y_i are summed over the warp's rows per column in FP64 (fixed xor
-    // pattern) and added to the warp's row of `red`.
-    constexpr int LB = CPL * (int)sizeof(T);
-    constexpr int U = (POLAR_SELL_BYTES / LB) > 1 ? (POLAR_SELL_BYTES / LB) : 1;
+    // light rows in sliced ELL.  The row's own entries are read after its gathers; d.v
+    // leaves the registers: after each slice the products x_i y_i are summed over the
+    // warp's rows per column in FP64 (fixed xor pattern) and added to the warp's row of red.
     constexpr int DC = CPL < 4 ? CPL : 4;  // columns per FP64 reduction pass
-    const int wid = blockIdx.x * kWarps + warp;
-    const int nw = gridDim.x * kWarps;
-    const int grp = lane / rg.G;
-    const int S = gpw;
-    int off_n = 0, end_n = 0, row_n = -1;
-    if (wid < g.nsl) {
-      off_n = __ldg(g.d_sl_off + wid);
-      end_n = __ldg(g.d_sl_off + wid + 1);
-      row_n = __ldg(g.d_sl_rows + (size_t)wid * S + grp);
-    }
-    for (int sl = wid; sl < g.nsl; sl += nw) {
-      const int off = off_n, w = (end_n - off_n) / S, row = row_n;
-      const int sn = sl + nw;
-      if (sn < g.nsl) {
-        off_n = __ldg(g.d_sl_off + sn);
-        end_n = __ldg(g.d_sl_off + sn + 1);
-        row_n = __ldg(g.d_sl_rows + (size_t)sn * S + grp);
-      }
-      const bool valid = row >= 0;
-      const bool go = valid && on;
-      A acc[CPL];
-#pragma unroll
-      for (int v = 0; v < CPL; ++v) acc[v] = A(0);
-      int deg = 0;
-      const int* sp = g.d_sl_idx + off + grp;
-      for (int k = 0; k < w; k += U) {
-        int jj[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) jj[u] = (k + u < w) ? ld_hint_i32(sp + (size_t)(k + u) * S, pol_stream) : -1;
-        T xv[U][CPL];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (go && jj[u] >= 0)
-            vload_hint<T, CPL>(xv[u], P.d + (size_t)jj[u] * ld + rg.col, row_policy(P, jj[u], pol_hot, pol_cold));
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-          if (jj[u] >= 0) {
-            ++deg;
-            if (go)
-#pragma unroll
-              for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
-          }
-      }
-      // y_i = (deg + sigma + added + shift) x_i - acc, formed in place in acc
+    sell_slice_pass<T, CPL, A>(g, rg, wid, nw, P.d, ld, on, hp, [&](int row, int deg, auto& acc, bool go) {
+      // y_i = (deg + sigma + shift) x_i - acc, formed in place in acc
       T xi[CPL];
       if (go) {
-        vload_hint<T, CPL>(xi, P.d + (size_t)row * ld + rg.col, row_policy(P, row, pol_hot, pol_cold));
+        vload_hint<T, CPL>(xi, P.d + (size_t)row * ld + rg.col, hp.row(row));
         const double dg = (double)deg + g.sigma + shift;
         T yv[CPL];
 #pragma unroll
         for (int v = 0; v < CPL; ++v) yv[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
-        vstore_hint<T, CPL>(P.v + (size_t)row * ld + rg.col, yv, pol_stream);
+        vstore_hint<T, CPL>(P.v + (size_t)row * ld + rg.col, yv, hp.stream);
 #pragma unroll
         for (int v = 0; v < CPL; ++v) acc[v] = (A)yv[v];
       }
@@ -404,7 +277,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
 #pragma unroll
           for (int v = 0; v < DC; ++v) wred[rg.col + v0 + v] += pr[v];
       }
-    }
+    });
     reduce_red_to_part(red, ld, P.part + (size_t)blockIdx.x * ld);
   } else {
     // MODE 2: light rows, one row group per row; the row's own entries are loaded with its

@@ -1,0 +1,193 @@
+// Sliced-ELL CSR-Laplacian SpMM passes shared by the solver's SpMM (mk_spmm) and the
+// standalone operator apply (polar_spmm) on unweighted graphs (sm_100a).
+//
+// A launch runs the heavy-row chunks first and then the slices of light rows:
+//  * heavy rows (degree above the partition's threshold) are cut into chunks of at most
+//    kChunkMax neighbours, one warp per chunk.  The warp stages the chunk's indices in
+//    shared memory with one coalesced pass; row group grp then takes neighbours grp,
+//    grp + gpw, ... in batches of independent gathers, and the groups combine by shuffles
+//    in a fixed pattern.  A row held in one chunk is finished by the warp; longer rows leave
+//    per-chunk partials that the last chunk to arrive sums in chunk order, so results do
+//    not depend on scheduling;
+//  * light rows come in slices of gpw degree-sorted rows (the graph's sl_* arrays): a
+//    warp reads neighbour k of all its rows with one coalesced load and issues predicated
+//    gather batches, so short rows have all their gathers in flight; the next slice's
+//    descriptors are fetched while this one is gathered, and a row's degree is the count
+//    of its valid entries.
+// Row sums are accumulated in A (FP64 for FP32 vectors unless the build says otherwise).
+// The caller finishes rows through callbacks, which is where the solver forms d.v and the
+// standalone apply adds the greedy's added edges.
+#pragma once
+#include "graph_ops.cuh"
+
+#ifndef POLAR_HEAVY_BYTES
+#define POLAR_HEAVY_BYTES 64  // bytes of gathered rows in flight per lane in a heavy chunk
+#endif
+#ifndef POLAR_SELL_BYTES
+#define POLAR_SELL_BYTES 64   // same for a slice of light rows
+#endif
+
+namespace polar {
+
+// L2 policies of one pass: rows below hot_rows are the most gathered rows of a
+// degree-ordered graph (kept with evict_last), the rest `cold`; `stream` for data read or
+// written once.
+struct GatherHints {
+  uint64_t hot, cold, stream;
+  int hot_rows;
+  POLAR_D uint64_t row(long long i) const { return i < hot_rows ? hot : cold; }
+};
+
+// mode 0: no hints (evict_normal everywhere); 1: hot rows evict_last, streams evict_first;
+// 2: as 1 with cold gathers evict_first.
+POLAR_D GatherHints make_gather_hints(int mode, int hot_rows) {
+  GatherHints h;
+  h.hot = l2_policy(mode ? 1 : 0);
+  h.cold = l2_policy(mode == 2 ? 2 : 0);
+  h.stream = l2_policy(mode ? 2 : 0);
+  h.hot_rows = hot_rows;
+  return h;
+}
+
+// Heavy chunks [wid, wid + nw, ...).  X rows have stride ldx; chunk partials have stride ldp.
+// single(i, deg, acc, xi): a row held in one chunk (row-group leader lanes, grp == 0);
+// partial(i, first, acc, xi): after a multi-chunk row's partial is stored (grp == 0, on);
+// fin(i, deg, sum): the last-arriving chunk with the row's combined sum (grp == 0).
+// xi is row i's own entries (loaded for grp == 0 when on).  s_idx: this warp's kChunkMax ints.
+template <typename T, int CPL, bool W, typename A, typename Single, typename Partial, typename Final>
+POLAR_D void heavy_chunk_pass(const polar_graph& g, const RowGroup& rg, int wid, int nw, const T* X, int ldx, int ldp,
+                              bool on, int* s_idx, A* chunk_part, int* hcount, const GatherHints& hp,
+                              Single&& single, Partial&& partial, Final&& fin) {
+  constexpr int LB = CPL * (int)sizeof(T);
+  constexpr int U = (POLAR_HEAVY_BYTES / LB) > 1 ? (POLAR_HEAVY_BYTES / LB) : 1;
+  const int lane = threadIdx.x & 31;
+  const int gpw = 32 / rg.G;
+  const int grp = lane / rg.G;
+  for (int ch = wid; ch < g.nchunks; ch += nw) {
+    const int h = __ldg(g.d_chunk_row + ch);
+    const int lo = __ldg(g.d_chunk_lo + ch), hi = __ldg(g.d_chunk_hi + ch);
+    const int i = __ldg(g.d_hrow + h);
+    const int c0 = __ldg(g.d_hchunk_off + h), c1 = __ldg(g.d_hchunk_off + h + 1);
+    const bool one = (c1 - c0) == 1;
+    T xi[CPL];
+    if (on && grp == 0) vload<T, CPL>(xi, X + (size_t)i * ldx + rg.col);
+    const int cnt = hi - lo;
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < kChunkMax / 32; ++q) {
+      const int k = 32 * q + lane;
+      if (k < cnt) s_idx[k] = ld_hint_i32(g.d_indices + lo + k, hp.stream);
+    }
+    __syncwarp();
+    A acc[CPL];
+#pragma unroll
+    for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+    const int nu = cnt > grp ? (cnt - grp + gpw - 1) / gpw : 0;
+    const int numax = (cnt + gpw - 1) / gpw;
+    for (int u0 = 0; u0 < numax; u0 += U) {
+      T xv[U][CPL];
+      A wv[U];
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (on && u0 + uu < nu) {
+          const int t = grp + gpw * (u0 + uu);
+          const int j = s_idx[t];
+          vload_hint<T, CPL>(xv[uu], X + (size_t)j * ldx + rg.col, hp.row(j));
+          wv[uu] = W ? (A)__ldg(g.d_wts + lo + t) : A(1);
+        }
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (on && u0 + uu < nu) {
+#pragma unroll
+          for (int v = 0; v < CPL; ++v) acc[v] = W ? fma(wv[uu], (A)xv[uu][v], acc[v]) : acc[v] + (A)xv[uu][v];
+        }
+    }
+    for (int o = rg.G; o < 32; o <<= 1)
+#pragma unroll
+      for (int v = 0; v < CPL; ++v) acc[v] += __shfl_xor_sync(0xffffffffu, acc[v], o);
+    if (one) {
+      if (grp == 0) single(i, cnt, acc, xi);
+      continue;
+    }
+    if (on && grp == 0) {
+      vstore<A, CPL>(chunk_part + (size_t)ch * ldp + rg.col, acc);
+      partial(i, ch == c0, acc, xi);
+    }
+    __threadfence();
+    __syncwarp();
+    int old = 0;
+    if (lane == 0) old = atomicAdd(hcount + h, 1);
+    old = __shfl_sync(0xffffffffu, old, 0);
+    if (old == c1 - c0 - 1 && grp == 0) {
+      __threadfence();
+      A sum[CPL];
+#pragma unroll
+      for (int v = 0; v < CPL; ++v) sum[v] = A(0);
+      if (on)
+        for (int c2 = c0; c2 < c1; ++c2) {
+          A pv[CPL];
+          vload_cg<A, CPL>(pv, chunk_part + (size_t)c2 * ldp + rg.col);
+#pragma unroll
+          for (int v = 0; v < CPL; ++v) sum[v] += pv[v];
+        }
+      const int deg = __ldg(g.d_indptr + i + 1) - __ldg(g.d_indptr + i);
+      fin(i, deg, sum);
+      if (lane == 0) hcount[h] = 0;
+    }
+    __syncwarp();
+  }
+}
+
+// Slices [wid, wid + nw, ...) of the light rows (g.sell_s == 32 / rg.G rows each).
+// row_end(row, deg, acc, go) is called by EVERY lane once per slice (it may shuffle):
+// row = this row group's row (-1 for a pad), go = a real row and on.
+template <typename T, int CPL, typename A, typename RowEnd>
+POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, int nw, const T* X, int ldx, bool on,
+                             const GatherHints& hp, RowEnd&& row_end) {
+  constexpr int LB = CPL * (int)sizeof(T);
+  constexpr int U = (POLAR_SELL_BYTES / LB) > 1 ? (POLAR_SELL_BYTES / LB) : 1;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / rg.G;
+  const int S = 32 / rg.G;
+  int off_n = 0, end_n = 0, row_n = -1;
+  if (wid < g.nsl) {
+    off_n = __ldg(g.d_sl_off + wid);
+    end_n = __ldg(g.d_sl_off + wid + 1);
+    row_n = __ldg(g.d_sl_rows + (size_t)wid * S + grp);
+  }
+  for (int sl = wid; sl < g.nsl; sl += nw) {
+    const int off = off_n, w = (end_n - off_n) / S, row = row_n;
+    const int sn = sl + nw;
+    if (sn < g.nsl) {
+      off_n = __ldg(g.d_sl_off + sn);
+      end_n = __ldg(g.d_sl_off + sn + 1);
+      row_n = __ldg(g.d_sl_rows + (size_t)sn * S + grp);
+    }
+    const bool go = row >= 0 && on;
+    A acc[CPL];
+#pragma unroll
+    for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+    int deg = 0;
+    const int* sp = g.d_sl_idx + off + grp;
+    for (int k = 0; k < w; k += U) {
+      int jj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) jj[u] = (k + u < w) ? ld_hint_i32(sp + (size_t)(k + u) * S, hp.stream) : -1;
+      T xv[U][CPL];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (go && jj[u] >= 0) vload_hint<T, CPL>(xv[u], X + (size_t)jj[u] * ldx + rg.col, hp.row(jj[u]));
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (jj[u] >= 0) {
+          ++deg;
+          if (go)
+#pragma unroll
+            for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
+        }
+    }
+    row_end(row, deg, acc, go);
+  }
+}
+
+}  // namespace polar

@@ -12,7 +12,6 @@ constexpr int kMaxLd = 128;
 constexpr int kHist = 16;  // M: iterations per deferred shifted-update pass
 constexpr int kNC = 2 + 2 * kHist;     // composed coefficients per (pole, column)
 constexpr int kMaxHeavyCtas = 1024;    // bound of the heavy-row launch (partials buffer rows)
-constexpr int kChunkMax = 256;         // neighbours per heavy-row chunk (the graph partition's CHUNK)
 #ifndef POLAR_E32
 #define POLAR_E32 2  // active rows per thread in the deferred update, FP32 iterates
 #endif

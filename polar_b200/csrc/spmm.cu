@@ -8,6 +8,7 @@
 #include "common.cuh"
 #include "graph_ops.cuh"
 #include "host_util.h"
+#include "sell_spmm.cuh"
 
 namespace polar {
 
@@ -86,6 +87,90 @@ __global__ void __launch_bounds__(512, POLAR_PANEL_MINB) spmm_panel_kernel(polar
   spmm_phase<T, VEC, WEIGHTED, false>(g, R, shift, X, Y, ldy, part, hcount, nullptr, nullptr);
 }
 
+// Sliced-ELL path (unweighted graphs with the layout for this width): the solver's SpMM
+// passes with the standalone row finish (diagonal, shift and the greedy's added edges per
+// row), FP64 row sums, the same L2 policies.  R == ld, a power of two.
+template <typename T, int CPL>
+__global__ void __launch_bounds__(512, 2) spmm_sell_kernel(polar_graph g, int ld, double shift, const T* X,
+                                                           int ldx, T* Y, int ldy, double* part, int* hcount,
+                                                           int l2_mode, int hot_rows) {
+  using A = double;
+  __shared__ int s_idx[16][kChunkMax];
+  const RowGroup rg = make_row_group<CPL>(ld);
+  const int warp = threadIdx.x >> 5;
+  const int wid = blockIdx.x * 16 + warp;
+  const int nw = gridDim.x * 16;
+  const GatherHints hp = make_gather_hints(l2_mode, hot_rows);
+  heavy_chunk_pass<T, CPL, false, A>(
+      g, rg, wid, nw, X, ldx, ld, true, s_idx[warp], part, hcount, hp,
+      [&](int i, int cnt, auto& acc, auto& xi) {
+        T yi[CPL];
+        finish_row_pre<T, CPL, true, A>(g, rg, i, cnt, shift, X, ldx, acc, Y, ldy, xi, yi, true);
+      },
+      [&](int, bool, auto&, auto&) {},
+      [&](int i, int deg, auto& sum) {
+        T xf[CPL], yi[CPL];
+        finish_row<T, CPL, true, A>(g, rg, i, deg, shift, X, ldx, sum, Y, ldy, xf, yi, true);
+      });
+  sell_slice_pass<T, CPL, A>(g, rg, wid, nw, X, ldx, true, hp, [&](int row, int deg, auto& acc, bool go) {
+    if (!go) return;
+    T xi[CPL];
+    vload_hint<T, CPL>(xi, X + (size_t)row * ldx + rg.col, hp.row(row));
+    const double wadd = added_terms<T, CPL, A>(g, rg, row, X, ldx, acc);
+    const double dg = (double)deg + g.sigma + wadd + shift;
+    T yv[CPL];
+#pragma unroll
+    for (int v = 0; v < CPL; ++v) yv[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
+    vstore_hint<T, CPL>(Y + (size_t)row * ldy + rg.col, yv, hp.stream);
+  });
+}
+
+template <typename T, int CPL>
+static int launch_spmm_sell(const polar_graph& g, int ld, double shift, const void* X, int ldx, void* Y, int ldy,
+                            void* scratch, int precision, cudaStream_t st) {
+  double* part = reinterpret_cast<double*>(scratch);
+  int* hcount = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + spmm_counter_offset(&g, precision));
+  int dev = 0, sms = 0, nb = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, spmm_sell_kernel<T, CPL>, 512, 0);
+  if (nb < 1) nb = 1;
+  const long long hot = (long long)(l2_hot_bytes_setting() / ((size_t)ld * sizeof(T)));
+  spmm_sell_kernel<T, CPL><<<nb * sms, 512, 0, st>>>(g, ld, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount,
+                                                      l2_mode_setting(), (int)(hot < g.n ? hot : g.n));
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_cuda_error("spmm launch", e);
+  return POLAR_OK;
+}
+
+// The sliced-ELL launch for this call, or nothing (used = false) when the row-loop
+// kernels apply: weighted graphs, no layout for this width, widths that are not a power of
+// two, or blocks that are not 16-byte aligned.
+template <typename T>
+static int try_spmm_sell(const polar_graph& g, int precision, int R, double shift, const void* X, int ldx, void* Y,
+                         int ldy, void* scratch, cudaStream_t st, bool* used) {
+  *used = false;
+  const int vmin = 16 / (int)sizeof(T);  // one 16-byte vector per lane at least
+  if (g.d_wts || g.nsl <= 0 || R < vmin || (R & (R - 1)) != 0) return POLAR_OK;
+  const int lanes = mk_spmm_lanes(precision, R);
+  const int cpl = R / lanes;
+  if (g.sell_s != 32 / lanes) return POLAR_OK;
+  const size_t es = sizeof(T);
+  if ((uintptr_t)X % 16 || (uintptr_t)Y % 16 || ((size_t)ldx * es) % 16 || ((size_t)ldy * es) % 16) return POLAR_OK;
+  *used = true;
+  switch (cpl) {
+    case 2: return launch_spmm_sell<T, 2>(g, R, shift, X, ldx, Y, ldy, scratch, precision, st);
+    case 4: return launch_spmm_sell<T, 4>(g, R, shift, X, ldx, Y, ldy, scratch, precision, st);
+    case 8: return launch_spmm_sell<T, 8>(g, R, shift, X, ldx, Y, ldy, scratch, precision, st);
+    case 16:
+      if (sizeof(T) == 4) return launch_spmm_sell<T, 16>(g, R, shift, X, ldx, Y, ldy, scratch, precision, st);
+      break;
+  }
+  *used = false;
+  return POLAR_OK;
+}
+
 static int spmm_vec(int precision, int R, int ldx, int ldy, const void* X, const void* Y) {
   const int maxv = precision == POLAR_MIXED ? 4 : 2;
   const size_t es = precision == POLAR_MIXED ? 4 : 8;
@@ -103,7 +188,7 @@ static int launch_spmm_panel(const polar_graph& g, int R, double shift, const vo
   using A = typename AccOf<T>::type;
   A* part = reinterpret_cast<A*>(scratch);
   int* hcount = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) +
-                                       (((size_t)(g.nchunks > 0 ? g.nchunks : 1) * 128 * sizeof(A) + 255) & ~size_t(255)));
+                                       spmm_counter_offset(&g, sizeof(T) == 4 ? POLAR_MIXED : POLAR_FP64));
   int dev = 0, sms = 0, nb = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -124,7 +209,7 @@ static int launch_spmm(const polar_graph& g, int R, double shift, const void* X,
   const int ldp = G * VEC;
   A* part = reinterpret_cast<A*>(scratch);
   int* hcount = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) +
-                                       (((size_t)(g.nchunks > 0 ? g.nchunks : 1) * 128 * sizeof(A) + 255) & ~size_t(255)));
+                                       spmm_counter_offset(&g, sizeof(T) == 4 ? POLAR_MIXED : POLAR_FP64));
   (void)ldp;
   const int gpb = (kSpmmBlock / 32) * (32 / G);
   long long groups_needed = (long long)g.n + g.nchunks;
@@ -149,8 +234,8 @@ using namespace polar;
 namespace polar {
 
 size_t spmm_counter_offset(const polar_graph* g, int precision) {
-  const size_t es = precision == POLAR_MIXED ? 4 : 8;
-  return ((size_t)(g->nchunks > 0 ? g->nchunks : 1) * 128 * es + 255) & ~size_t(255);
+  (void)precision;  // chunk partials: up to 128 columns of FP64 row sums in either precision
+  return ((size_t)(g->nchunks > 0 ? g->nchunks : 1) * 128 * 8 + 255) & ~size_t(255);
 }
 
 int spmm_check_args(const polar_graph* g, int precision, int R, const void* d_X, int ldx, const void* d_Y,
@@ -190,6 +275,13 @@ extern "C" int polar_spmm(const polar_graph* g, int precision, int R, double shi
   const int vec = spmm_vec(precision, R, ldx, ldy, d_X, d_Y);
   const bool w = g->d_wts != nullptr;
   cudaStream_t st = (cudaStream_t)stream;
+  {
+    bool used = false;
+    const int rs = precision == POLAR_MIXED
+                       ? try_spmm_sell<float>(*g, precision, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st, &used)
+                       : try_spmm_sell<double>(*g, precision, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st, &used);
+    if (used || rs != POLAR_OK) return rs;
+  }
   const bool pow2 = (R & (R - 1)) == 0;
   if (pow2 && ldx == R && precision == POLAR_MIXED && vec == 4)
     return w ? launch_spmm_panel<float, 4, true>(*g, R, shift, d_X, ldx, d_Y, ldy, d_scratch, st)

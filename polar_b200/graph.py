@@ -344,9 +344,9 @@ class Op:
         prec = _lib.POLAR_MIXED if X.dtype == torch.float32 else _lib.POLAR_FP64
         maxc = 128 if prec == _lib.POLAR_MIXED else 64
         Y = torch.empty_like(X)
-        g = self.struct()
         lib = _lib.load()
         stream = torch.cuda.current_stream(X.device).cuda_stream
+        g = self.struct()
         key = (prec, X.device.index)
         if key not in self._scratch:
             nb = lib.polar_spmm_scratch_bytes(g, prec, maxc)
@@ -358,6 +358,9 @@ class Op:
             hi = min(R, lo + maxc)
             xs = X[:, lo:hi]
             ys = Y[:, lo:hi]
-            _lib.check(lib.polar_spmm(g, prec, hi - lo, float(shift), xs.data_ptr(), R, ys.data_ptr(), R,
+            # unweighted graphs: the sliced-ELL layout of the solver for this width (the
+            # library uses it when the width is a power of two)
+            gw = self.struct(sell_rows=lib.polar_sell_rows(prec, hi - lo)) if not self.G.weighted else g
+            _lib.check(lib.polar_spmm(gw, prec, hi - lo, float(shift), xs.data_ptr(), R, ys.data_ptr(), R,
                                       scratch.data_ptr(), stream), "polar_spmm")
         return Y.reshape(-1) if squeeze else Y
