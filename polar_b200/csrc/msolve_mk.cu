@@ -252,11 +252,9 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
     // leaves the registers: after each slice the products x_i y_i are summed over the
     // warp's rows per column in FP64 (fixed xor pattern) and added to the warp's row of red.
     constexpr int DC = CPL < 4 ? CPL : 4;  // columns per FP64 reduction pass
-    sell_slice_pass<T, CPL, A>(g, rg, wid, nw, P.d, ld, on, hp, [&](int row, int deg, auto& acc, bool go) {
+    sell_slice_pass<T, CPL, A>(g, rg, wid, nw, P.d, ld, on, hp, [&](int row, int deg, auto& acc, auto& xi, bool go) {
       // y_i = (deg + sigma + shift) x_i - acc, formed in place in acc
-      T xi[CPL];
       if (go) {
-        vload_hint<T, CPL>(xi, P.d + (size_t)row * ld + rg.col, hp.row(row));
         const double dg = (double)deg + g.sigma + shift;
         T yv[CPL];
 #pragma unroll
@@ -465,7 +463,9 @@ __global__ void __launch_bounds__(kBlock, POLAR_STREAM_MINB) mk_dir(const __grid
 
 // ---- deferred shifted update (final pass writes the output) -----------------------------
 template <typename T, int E>
-__global__ void __launch_bounds__(kBlock, 2) mk_flush(const __grid_constant__ SolvePrm<T> P, int force_final) {
+// One resident CTA per SM: the composed coefficients of a column chunk take up to ~150 KB
+// of shared memory, so the launch bound leaves the registers to the double-buffered rows.
+__global__ void __launch_bounds__(kBlock, 1) mk_flush(const __grid_constant__ SolvePrm<T> P, int force_final) {
   extern __shared__ __align__(16) unsigned char flush_sm[];
 
   pdl_wait();

@@ -139,8 +139,12 @@ POLAR_D void heavy_chunk_pass(const polar_graph& g, const RowGroup& rg, int wid,
 }
 
 // Slices [wid, wid + nw, ...) of the light rows (g.sell_s == 32 / rg.G rows each).
-// row_end(row, deg, acc, go) is called by EVERY lane once per slice (it may shuffle):
-// row = this row group's row (-1 for a pad), go = a real row and on.
+// row_end(row, deg, acc, xi, go) is called by EVERY lane once per slice (it may shuffle):
+// row = this row group's row (-1 for a pad), xi = its own entries (valid when go),
+// go = a real row and on.
+// Latency: a slice's work is a chain index load -> gathers -> accumulate per batch, so the
+// indices of the next batch (or of the next slice's first batch) are loaded while this
+// batch's gathers are in flight, and the row's own entries are loaded at the slice start.
 template <typename T, int CPL, typename A, typename RowEnd>
 POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, int nw, const T* X, int ldx, bool on,
                              const GatherHints& hp, RowEnd&& row_end) {
@@ -149,34 +153,48 @@ POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, 
   const int lane = threadIdx.x & 31;
   const int grp = lane / rg.G;
   const int S = 32 / rg.G;
-  int off_n = 0, end_n = 0, row_n = -1;
+  // descriptors (offset, width, row) of the current and the next slice, and the index
+  // batch queued for the current slice
+  int off = 0, w = 0, row = -1;
+  int jj[U];
+  auto fetch_desc = [&](int sl, int& o, int& wd, int& r) {
+    o = __ldg(g.d_sl_off + sl);
+    wd = (__ldg(g.d_sl_off + sl + 1) - o) / S;
+    r = __ldg(g.d_sl_rows + (size_t)sl * S + grp);
+  };
+  auto fetch_idx = [&](int o, int wd, int k, int (&dst)[U]) {
+    const int* sp = g.d_sl_idx + o + grp;
+#pragma unroll
+    for (int u = 0; u < U; ++u) dst[u] = (k + u < wd) ? ld_hint_i32(sp + (size_t)(k + u) * S, hp.stream) : -1;
+  };
   if (wid < g.nsl) {
-    off_n = __ldg(g.d_sl_off + wid);
-    end_n = __ldg(g.d_sl_off + wid + 1);
-    row_n = __ldg(g.d_sl_rows + (size_t)wid * S + grp);
+    fetch_desc(wid, off, w, row);
+    fetch_idx(off, w, 0, jj);
   }
   for (int sl = wid; sl < g.nsl; sl += nw) {
-    const int off = off_n, w = (end_n - off_n) / S, row = row_n;
     const int sn = sl + nw;
-    if (sn < g.nsl) {
-      off_n = __ldg(g.d_sl_off + sn);
-      end_n = __ldg(g.d_sl_off + sn + 1);
-      row_n = __ldg(g.d_sl_rows + (size_t)sn * S + grp);
-    }
+    int off_n = 0, w_n = 0, row_n = -1;
+    if (sn < g.nsl) fetch_desc(sn, off_n, w_n, row_n);
     const bool go = row >= 0 && on;
+    T xi[CPL];
+    if (go) vload_hint<T, CPL>(xi, X + (size_t)row * ldx + rg.col, hp.row(row));
     A acc[CPL];
 #pragma unroll
     for (int v = 0; v < CPL; ++v) acc[v] = A(0);
     int deg = 0;
-    const int* sp = g.d_sl_idx + off + grp;
     for (int k = 0; k < w; k += U) {
-      int jj[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) jj[u] = (k + u < w) ? ld_hint_i32(sp + (size_t)(k + u) * S, hp.stream) : -1;
       T xv[U][CPL];
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (go && jj[u] >= 0) vload_hint<T, CPL>(xv[u], X + (size_t)jj[u] * ldx + rg.col, hp.row(jj[u]));
+      int jn[U];
+      if (k + U < w)
+        fetch_idx(off, w, k + U, jn);
+      else if (sn < g.nsl)
+        fetch_idx(off_n, w_n, 0, jn);
+      else
+#pragma unroll
+        for (int u = 0; u < U; ++u) jn[u] = -1;
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (jj[u] >= 0) {
@@ -185,8 +203,14 @@ POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, 
 #pragma unroll
             for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];
         }
+#pragma unroll
+      for (int u = 0; u < U; ++u) jj[u] = jn[u];
     }
-    row_end(row, deg, acc, go);
+    if (w == 0 && sn < g.nsl) fetch_idx(off_n, w_n, 0, jj);
+    row_end(row, deg, acc, xi, go);
+    off = off_n;
+    w = w_n;
+    row = row_n;
   }
 }
 

@@ -433,10 +433,21 @@ POLAR_D void shifted_update_smem(const SolvePrm<T>& P, int nsteps, bool first, b
 //   X <- X + alpha P + sum_k gamma_k h_k,   P <- beta P + sum_k delta_k h_k
 // (2 + 2M fused multiply-adds, no per-step branches; unused steps have zero coefficients
 // and the history is zeroed per solve).  CTA = 128-byte column chunk as above; the chunk's
-// coefficients of all poles (p x kNC x CW) are staged in shared memory as T.
+// coefficients of all poles are staged in shared memory as T, one row per (pole, column).
+//
+// Shared-memory row of one (pole, column) in the composed flush: gamma_k, delta_k
+// interleaved for k = 0..M-1, then alpha, beta; padded so that a lane's row starts 16-byte
+// aligned and the rows of 8 consecutive lanes fall on distinct banks (36 floats, 34 doubles:
+// 4-word lane stride mod 32), which makes every coefficient read one conflict-free 128-bit
+// shared load of two (FP32) or one (FP64) history steps' pair.
+template <typename T>
+POLAR_HD constexpr int composed_row() {
+  return sizeof(T) == 4 ? 36 : 34;
+}
+
 template <typename T>
 POLAR_HD size_t composed_smem_bytes(int ld, int p) {
-  return (size_t)p * kNC * flush_cw<T>(ld) * sizeof(T);
+  return (size_t)p * flush_cw<T>(ld) * composed_row<T>() * sizeof(T);
 }
 
 #ifndef POLAR_FLUSH_F64
@@ -463,12 +474,17 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
   const int rows_per_pass = blockDim.x / cw;
   const int TR = rows_per_pass * E;
   const int c = cc * cw + cl;
+  // composed coefficients of this CTA's columns, in the composed_row layout: source t = 0
+  // alpha, 1 beta, 2 + k gamma_k, 2 + M + k delta_k
+  constexpr int NR = composed_row<T>();
   const int total = p * kNC * cw;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    const int l = i % cw;
-    const int jt = i / cw;  // j * kNC + t
-    const int j = jt / kNC, t = jt % kNC;
-    sm[i] = (T)P.cmp[((size_t)j * ld + cc * cw + l) * kNC + t];
+    const int t = i % kNC;
+    const int jl = i / kNC;  // j * cw + l
+    const int j = jl / cw, l = jl % cw;
+    const int dst = t == 0 ? 2 * kHist : t == 1 ? 2 * kHist + 1
+                  : t < 2 + kHist ? 2 * (t - 2) : 2 * (t - 2 - kHist) + 1;
+    sm[(size_t)jl * NR + dst] = (T)P.cmp[((size_t)j * ld + cc * cw + l) * kNC + t];
   }
   __syncthreads();
   const int ntile = (nA + TR - 1) / TR;
@@ -502,8 +518,11 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
     auto apply = [&](int j, T (&x)[E], T (&pv)[E], bool on) {
       if (!first && !final_pass && !on) return;
       if (on) {
-        const T* cf = sm + (size_t)j * kNC * cw + cl;
-        const C alpha = (C)cf[0], beta = (C)cf[cw];
+        const T* cf = sm + ((size_t)j * cw + cl) * NR;
+        constexpr int V = 16 / (int)sizeof(T);  // coefficients per 128-bit shared load
+        VecU<T, 2> ab;
+        ab.v = *reinterpret_cast<const typename VecType<T, 2>::type*>(cf + 2 * kHist);
+        const C alpha = (C)ab.a[0], beta = (C)ab.a[1];
         C xc[E], pc[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -512,12 +531,18 @@ POLAR_D void shifted_update_composed(const SolvePrm<T>& P, int nsteps, bool firs
           pc[e] = beta * p0;
         }
 #pragma unroll
-        for (int k = 0; k < kHist; ++k) {
-          const C gk = (C)cf[(2 + k) * cw], dk = (C)cf[(2 + kHist + k) * cw];
+        for (int k0 = 0; k0 < 2 * kHist; k0 += V) {
+          VecU<T, V> q;
+          q.v = *reinterpret_cast<const typename VecType<T, V>::type*>(cf + k0);
 #pragma unroll
-          for (int e = 0; e < E; ++e) {
-            xc[e] = fma(gk, (C)hv[e][k], xc[e]);
-            pc[e] = fma(dk, (C)hv[e][k], pc[e]);
+          for (int u = 0; u < V; u += 2) {
+            const int k = (k0 + u) / 2;
+            const C gk = (C)q.a[u], dk = (C)q.a[u + 1];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+              xc[e] = fma(gk, (C)hv[e][k], xc[e]);
+              pc[e] = fma(dk, (C)hv[e][k], pc[e]);
+            }
           }
         }
 #pragma unroll

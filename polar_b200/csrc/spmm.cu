@@ -112,10 +112,8 @@ __global__ void __launch_bounds__(512, 2) spmm_sell_kernel(polar_graph g, int ld
         T xf[CPL], yi[CPL];
         finish_row<T, CPL, true, A>(g, rg, i, deg, shift, X, ldx, sum, Y, ldy, xf, yi, true);
       });
-  sell_slice_pass<T, CPL, A>(g, rg, wid, nw, X, ldx, true, hp, [&](int row, int deg, auto& acc, bool go) {
+  sell_slice_pass<T, CPL, A>(g, rg, wid, nw, X, ldx, true, hp, [&](int row, int deg, auto& acc, auto& xi, bool go) {
     if (!go) return;
-    T xi[CPL];
-    vload_hint<T, CPL>(xi, X + (size_t)row * ldx + rg.col, hp.row(row));
     const double wadd = added_terms<T, CPL, A>(g, rg, row, X, ldx, acc);
     const double dg = (double)deg + g.sigma + wadd + shift;
     T yv[CPL];
