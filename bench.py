@@ -163,24 +163,11 @@ def job_seconds(local_s, world, device):
 def build_inputs(a):
     """(n, N, k, edges, candidates, config) of the workload, generated from its seeds (or
     read from --cache, where a previous run left them)."""
-    from polar_b200.synth import CONFIGS, candidates, chung_lu
+    from polar_b200.synth import CONFIGS, make_config
     c = dict(CONFIGS[a.config])
-    n = a.n or c["n"]
-    N = a.N or c["N"]
     k = a.k or c["k"]
-    path = None
-    if a.cache:
-        os.makedirs(a.cache, exist_ok=True)
-        path = os.path.join(a.cache, f"{a.config}_n{n}_N{N}.npz")
-        if os.path.exists(path):
-            z = np.load(path)
-            return dict(n=n, N=N, k=k, E=z["edges"].astype(np.int64), cand=z["cand"].astype(np.int64), cfg=c)
-    E = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=c["dmax"] if n == c["n"] else None,
-                 min_degree=c.get("min_degree", 0))
-    cand = candidates(n, E, N, c["seed"] + 7919)
-    if path:
-        np.savez(path, edges=E.astype(np.int32), cand=cand.astype(np.int32))
-    return dict(n=n, N=N, k=k, E=E, cand=cand, cfg=c)
+    E, n, cand, c = make_config(a.config, n=a.n, N=a.N, cache=a.cache)
+    return dict(n=n, N=len(cand), k=k, E=E, cand=cand, cfg=c)
 
 
 # ---------------------------------------------------------------------------------------

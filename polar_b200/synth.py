@@ -180,14 +180,31 @@ def batch_specs(count=48, seed=3):
     return out
 
 
-def make_config(name, n=None, N=None, cand_seed=None):
-    """Build (edges, n, cand) for a named workload, optionally shrunk to `n` vertices
-    (mean degree and exponent kept) and `N` candidates."""
+def make_config(name, n=None, N=None, cand_seed=None, cache=None):
+    """Build (edges, n, cand, config) for a named workload, optionally shrunk to `n`
+    vertices (mean degree and exponent kept) and `N` candidates.
+
+    cache: a directory (default $POLAR_DATA when set) holding one .npz per (workload, n, N,
+    candidate seed), written on first use and read afterwards, as realworld/graphs.py:46-50
+    caches each prepared graph; the generation takes about a minute at 4M vertices."""
+    import os
     c = dict(CONFIGS[name])
     n = c["n"] if n is None else int(n)
     N = c["N"] if N is None else int(N)
+    seed = c["seed"] + 7919 if cand_seed is None else int(cand_seed)
+    cache = cache if cache is not None else os.environ.get("POLAR_DATA")
+    path = None
+    if cache:
+        os.makedirs(cache, exist_ok=True)
+        path = os.path.join(cache, f"{name}_n{n}_N{N}_s{seed}.npz")
+        if os.path.exists(path):
+            z = np.load(path)
+            return z["edges"].astype(np.int64), n, z["cand"].astype(np.int64), c
     dmax = c["dmax"] if n == c["n"] else None
     edges = chung_lu(n, c["mean_deg"], c["gamma"], c["seed"], dmax=dmax, min_degree=c.get("min_degree", 0))
-    seed = c["seed"] + 7919 if cand_seed is None else cand_seed
     cand = candidates(n, edges, N, seed)
+    if path:
+        tmp = path + ".tmp.npz"
+        np.savez(tmp, edges=edges.astype(np.int32), cand=cand.astype(np.int32))
+        os.replace(tmp, path)
     return edges, n, cand, c

@@ -251,3 +251,19 @@ int main() {
     c = out[4]
     assert c[5] == 148 and all(x >= 1 for x in c[:5])
     assert c[:5] == sorted(c[:5])                 # more cost, no fewer CTAs
+
+
+def test_candidates_batched_identity_and_cache(tmp_path):
+    """The batched pool equals the reference rule's one-pair-per-draw pool (the oracle's
+    restatement of realworld/graphs.py:61-69) at N = 10^5, and make_config's .npz cache
+    returns the generated workload unchanged."""
+    from oracle import polar_oracle as O
+    from polar_b200.synth import candidates, chung_lu, make_config
+    n = 317080
+    E = chung_lu(n, 6.6, 2.4, 1, min_degree=1)
+    np.testing.assert_array_equal(candidates(n, E, 100_000, 8), O.candidates(n, E, 100_000, 8))
+    E1, n1, c1, _ = make_config("precision-n317k", n=4000, N=3000, cache=str(tmp_path))
+    E2, n2, c2, _ = make_config("precision-n317k", n=4000, N=3000, cache=str(tmp_path))
+    assert len(list(tmp_path.iterdir())) == 1
+    np.testing.assert_array_equal(E1, E2)
+    np.testing.assert_array_equal(c1, c2)
