@@ -635,16 +635,21 @@ def run_solve(a):
                 for prec in ("mixed", "fp64"):
                     if prec == "fp64" and Wm.shape[1] > 64:
                         continue
-                    lib.polar_set_kernel_timing(1)
-                    try:
-                        S.msolve(op, Wm, tau, small[0], c["tol"], maxit=48, track=False, precision=prec,
-                                 active_pos=small[1])
-                    except _lib.PolarError as e:
-                        if e.status != _lib.POLAR_ERR_ITER_CAP:
-                            raise
-                    kt = _lib.kernel_timing()
-                    lib.polar_set_kernel_timing(0)
-                    row[f"{prec}_{name}"] = {k2: round(v[1] / max(1, v[0]), 4) for k2, v in kt.items() if v[0]}
+                    # lane widths: the solver's default, and 16 / 64 bytes at the bank width
+                    for lb in ((0,) if Wm.shape[1] <= 16 else (0, 16, 64)):
+                        lib.polar_set_spmm_lane_bytes(lb)
+                        lib.polar_set_kernel_timing(1)
+                        try:
+                            S.msolve(op, Wm, tau, small[0], c["tol"], maxit=48, track=False, precision=prec,
+                                     active_pos=small[1])
+                        except _lib.PolarError as e:
+                            if e.status != _lib.POLAR_ERR_ITER_CAP:
+                                raise
+                        kt = _lib.kernel_timing()
+                        lib.polar_set_kernel_timing(0)
+                        lib.polar_set_spmm_lane_bytes(0)
+                        key = f"{prec}_{name}" + (f"_lane{lb}" if lb else "")
+                        row[key] = {k2: round(v[1] / max(1, v[0]), 4) for k2, v in kt.items() if v[0]}
             out[pol] = row
         _lib.check(lib.polar_set_l2_policy(0, 64 << 20), "l2 policy")
         print(json.dumps({"workload": a.config, "quick": True, "n": n, "nnz": G.nnz,
