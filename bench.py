@@ -652,6 +652,23 @@ def run_solve(a):
                         row[key] = {k2: round(v[1] / max(1, v[0]), 4) for k2, v in kt.items() if v[0]}
             out[pol] = row
         _lib.check(lib.polar_set_l2_policy(0, 64 << 20), "l2 policy")
+        # heavy-row threshold of the shortlist width (mixed): rows above it go to warp chunks
+        from polar_b200 import autotune
+        thr = {}
+        for t in (16, 32, 64, 128):
+            autotune.record(G, "mixed", R, (0, 1, t))
+            lib.polar_set_kernel_timing(1)
+            try:
+                S.msolve(op, Wd, tau, small[0], c["tol"], maxit=48, track=False, precision="mixed",
+                         active_pos=small[1])
+            except _lib.PolarError as e:
+                if e.status != _lib.POLAR_ERR_ITER_CAP:
+                    raise
+            kt = _lib.kernel_timing()
+            lib.polar_set_kernel_timing(0)
+            thr[t] = round(kt["spmm"][1] / max(1, kt["spmm"][0]), 4)
+        autotune.clear(G)
+        out["heavy_thresh_mixed_R%d" % R] = thr
         print(json.dumps({"workload": a.config, "quick": True, "n": n, "nnz": G.nnz,
                           "ms_per_launch_by_l2_policy": out}), flush=True)
         return

@@ -54,6 +54,8 @@ POLAR_D bool last_cta(int* cnt) {
 }
 
 constexpr size_t kFlushSmemMax = 200 * 1024;
+// cp.async ring of the SpMM's slice pass per warp: stages x POLAR_SELL_BYTES x 32 lanes
+constexpr int kSellRingWarp = POLAR_SELL_STAGES * POLAR_SELL_BYTES * 32;
 
 POLAR_D bool solve_live(const int* ctl, const long long* stats, long long maxit) {
   return ld_volatile_i32(ctl + C_ANY) != 0 && stats[0] < maxit && ld_volatile_i32(ctl + C_ERR) == 0;
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
     // leaves the registers: after each slice the products x_i y_i are summed over the
     // warp's rows per column in FP64 (fixed xor pattern) and added to the warp's row of red.
     constexpr int DC = CPL < 4 ? CPL : 4;  // columns per FP64 reduction pass
-    sell_slice_pass<T, CPL, A>(g, rg, wid, nw, P.d, ld, on, hp, [&](int row, int deg, auto& acc, auto& xi, bool go) {
+    auto row_end = [&](int row, int deg, auto& acc, auto& xi, bool go) {
       // y_i = (deg + sigma + shift) x_i - acc, formed in place in acc
       if (go) {
         const double dg = (double)deg + g.sigma + shift;
@@ -275,7 +277,14 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
 #pragma unroll
           for (int v = 0; v < DC; ++v) wred[rg.col + v0 + v] += pr[v];
       }
-    });
+    };
+    if constexpr (POLAR_SELL_ASYNC != 0 && (CPL * sizeof(T)) % 16 == 0) {
+      extern __shared__ __align__(16) unsigned char spmm_ring[];
+      sell_slice_pass_async<T, CPL, A>(g, rg, wid, nw, P.d, ld, on, hp, spmm_ring + (size_t)warp * kSellRingWarp,
+                                       row_end);
+    } else {
+      sell_slice_pass<T, CPL, A>(g, rg, wid, nw, P.d, ld, on, hp, row_end);
+    }
     reduce_red_to_part(red, ld, P.part + (size_t)blockIdx.x * ld);
   } else {
     // MODE 2: light rows, one row group per row; the row's own entries are loaded with its
@@ -533,11 +542,39 @@ static bool spmm_merged(int cpl, const SolvePrm<T>& P) {
   return !W && P.g.nsl > 0 && P.g.sell_s == gpw;
 }
 
+// Dynamic shared memory of the merged SpMM launch: the slice pass's cp.async ring when it
+// is built in (the attribute is raised once per instantiation).
+template <typename T, int CPL>
+static size_t ring_bytes() {
+  if (POLAR_SELL_ASYNC == 0 || (CPL * sizeof(T)) % 16 != 0) return 0;
+  return (size_t)kWarps * kSellRingWarp;
+}
+
+template <typename T, int CPL, bool W>
+static void ring_attribute() {
+  static bool done = false;
+  if (!done && ring_bytes<T, CPL>() > 0) {
+    cudaFuncSetAttribute(mk_spmm<T, CPL, W, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)ring_bytes<T, CPL>());
+  }
+  done = true;
+}
+
 // SpMM launch for a runtime choice of columns per lane.
 template <typename T, bool W>
 struct SpmmLaunch {
   template <int CPL>
-  static int grid() { return occ_grid(mk_spmm<T, CPL, W, 2>, kBlock); }
+  static int grid() {
+    ring_attribute<T, CPL, W>();
+    int dev = 0, sms = 0, nb = 0, nb3 = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mk_spmm<T, CPL, W, 2>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb3, mk_spmm<T, CPL, W, 3>, kBlock, ring_bytes<T, CPL>());
+    if (nb3 < nb) nb = nb3;
+    if (nb < 1) nb = 1;
+    return nb * sms;
+  }
   // part 1: heavy-row launch, part 2: light-row launch
   template <int CPL>
   static void go(int part, int g, const SolvePrm<T>& P, cudaStream_t st) {
@@ -546,7 +583,7 @@ struct SpmmLaunch {
       return;
     }
     if (spmm_merged<T, W>(CPL, P))
-      launch_k(mk_spmm<T, CPL, W, 3>, g, kBlock, 0, st, P);
+      launch_k(mk_spmm<T, CPL, W, 3>, g, kBlock, ring_bytes<T, CPL>(), st, P);
     else
       launch_k(mk_spmm<T, CPL, W, 2>, g, kBlock, 0, st, P);
   }

@@ -27,7 +27,25 @@
 #define POLAR_SELL_BYTES 64   // same for a slice of light rows
 #endif
 
+#ifndef POLAR_SELL_ASYNC
+#define POLAR_SELL_ASYNC 0  // 1: the slice pass gathers through cp.async into shared memory
+#endif
+#ifndef POLAR_SELL_STAGES
+#define POLAR_SELL_STAGES 2  // batches of the cp.async ring per lane
+#endif
+
 namespace polar {
+
+// 16-byte asynchronous copy global -> shared (L2 only); src_bytes 0 fills zeros and reads
+// nothing.
+POLAR_D void cp_async16(void* smem, const void* gmem, int src_bytes, uint64_t pol) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;"
+               ::"r"(s), "l"(gmem), "r"(src_bytes), "l"(pol) : "memory");
+}
+POLAR_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+POLAR_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // L2 policies of one pass: rows below hot_rows are the most gathered rows of a
 // degree-ordered graph (kept with evict_last), the rest `cold`; `stream` for data read or
@@ -212,6 +230,114 @@ POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, 
     w = w_n;
     row = row_n;
   }
+}
+
+// The slice pass with its gathers in flight as cp.async copies into a per-lane ring in
+// shared memory (`ring`: this warp's POLAR_SELL_STAGES * U * 32 * LB bytes, laid out
+// [stage][u][lane] so that each batch is written and read conflict-free), so that no
+// register holds a gather in flight: the next batch (of this slice, or the next slice's
+// first) is issued before the current one is waited for and summed.  Each lane reads only
+// what it copied, so no barrier is needed; the sums are formed in the same order as
+// sell_slice_pass, so results are identical.
+template <typename T, int CPL, typename A, typename RowEnd>
+POLAR_D void sell_slice_pass_async(const polar_graph& g, const RowGroup& rg, int wid, int nw, const T* X, int ldx,
+                                   bool on, const GatherHints& hp, unsigned char* ring, RowEnd&& row_end) {
+  constexpr int LB = CPL * (int)sizeof(T);
+  constexpr int U = (POLAR_SELL_BYTES / LB) > 1 ? (POLAR_SELL_BYTES / LB) : 1;
+  constexpr int NC = LB / 16;  // 16-byte copies per lane per gathered row
+  constexpr int NS = POLAR_SELL_STAGES;
+  static_assert(LB % 16 == 0, "lane share of a row must be whole 16-byte copies");
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / rg.G;
+  const int S = 32 / rg.G;
+  auto slot = [&](int stage, int u, int c) -> unsigned char* {
+    return ring + ((size_t)((stage * U + u) * NC + c) * 32 + lane) * 16;
+  };
+  auto fetch_desc = [&](int sl, int& o, int& wd, int& r) {
+    o = __ldg(g.d_sl_off + sl);
+    wd = (__ldg(g.d_sl_off + sl + 1) - o) / S;
+    r = __ldg(g.d_sl_rows + (size_t)sl * S + grp);
+  };
+  auto fetch_idx = [&](int o, int wd, int k, int (&dst)[U]) {
+    const int* sp = g.d_sl_idx + o + grp;
+#pragma unroll
+    for (int u = 0; u < U; ++u) dst[u] = (k + u < wd) ? ld_hint_i32(sp + (size_t)(k + u) * S, hp.stream) : -1;
+  };
+  auto issue = [&](const int (&jj)[U], bool go, int stage) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool ok = go && jj[u] >= 0;
+      const T* src = ok ? X + (size_t)jj[u] * ldx + rg.col : X;
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        cp_async16(slot(stage, u, c), reinterpret_cast<const unsigned char*>(src) + 16 * c, ok ? 16 : 0,
+                   ok ? hp.row(jj[u]) : hp.stream);
+    }
+    cp_async_commit();
+  };
+  int off = 0, w = 0, row = -1;
+  int jj[U];
+  int stage = 0;
+  if (wid < g.nsl) {
+    fetch_desc(wid, off, w, row);
+    fetch_idx(off, w, 0, jj);
+    issue(jj, row >= 0 && on, 0);
+  }
+  for (int sl = wid; sl < g.nsl; sl += nw) {
+    const int sn = sl + nw;
+    int off_n = 0, w_n = 0, row_n = -1;
+    if (sn < g.nsl) fetch_desc(sn, off_n, w_n, row_n);
+    const bool go = row >= 0 && on;
+    T xi[CPL];
+    if (go) vload_hint<T, CPL>(xi, X + (size_t)row * ldx + rg.col, hp.row(row));
+    A acc[CPL];
+#pragma unroll
+    for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+    int deg = 0;
+    const int nb = w > 0 ? (w + U - 1) / U : 1;  // an empty slice still owns its one issued batch
+    for (int b = 0; b < nb; ++b) {
+      // issue the following batch: this slice's next, or the next slice's first
+      int jn[U];
+      const int nst = (stage + 1) % NS;
+      if (b + 1 < nb) {
+        fetch_idx(off, w, (b + 1) * U, jn);
+        issue(jn, go, nst);
+      } else if (sn < g.nsl) {
+        fetch_idx(off_n, w_n, 0, jn);
+        issue(jn, row_n >= 0 && on, nst);
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) jn[u] = -1;
+        cp_async_commit();  // empty group keeps one group per batch
+      }
+      cp_async_wait<1>();  // the current batch has landed
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (jj[u] >= 0) {
+          ++deg;
+          if (go) {
+            T xv[CPL];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+              VecU<T, 16 / (int)sizeof(T)> q;
+              q.v = *reinterpret_cast<const typename VecType<T, 16 / (int)sizeof(T)>::type*>(slot(stage, u, c));
+#pragma unroll
+              for (int e = 0; e < 16 / (int)sizeof(T); ++e) xv[c * (16 / (int)sizeof(T)) + e] = q.a[e];
+            }
+#pragma unroll
+            for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[v];
+          }
+        }
+#pragma unroll
+      for (int u = 0; u < U; ++u) jj[u] = jn[u];
+      stage = nst;
+    }
+    row_end(row, deg, acc, xi, go);
+    off = off_n;
+    w = w_n;
+    row = row_n;
+  }
+  cp_async_wait<0>();
 }
 
 }  // namespace polar

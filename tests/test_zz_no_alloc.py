@@ -27,7 +27,9 @@ def test_noalloc_matches_caller_scratch(prec, R):
     code = _lib.POLAR_FP64 if prec == "fp64" else _lib.POLAR_MIXED
     X = torch.as_tensor(np.random.default_rng(R).normal(size=(n, R)), dtype=dt, device="cuda")
     Y0 = op(X, 0.37)  # polar_spmm with scratch from the caller
-    g = op.struct()
+    # the graph struct op() hands to polar_spmm for this width (its sliced-ELL layout when
+    # R is a power of two), so both entry points run the same kernel
+    g = op.struct(sell_rows=lib.polar_sell_rows(code, R))
     stream = torch.cuda.current_stream().cuda_stream
     outs = []
     for _ in range(2):  # two calls in a row reuse the same fixed scratch
