@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(512, 2) spmm_sell_kernel(polar_graph g, int ld
         T xf[CPL], yi[CPL];
         finish_row<T, CPL, true, A>(g, rg, i, deg, shift, X, ldx, sum, Y, ldy, xf, yi, true);
       });
-  sell_slice_pass<T, CPL, A>(g, rg, wid, nw, X, ldx, true, hp, [&](int row, int deg, auto& acc, auto& xi, bool go) {
+  auto row_end = [&](int row, int deg, auto& acc, auto& xi, bool go) {
     if (!go) return;
     const double wadd = added_terms<T, CPL, A>(g, rg, row, X, ldx, acc);
     const double dg = (double)deg + g.sigma + wadd + shift;
@@ -120,7 +120,14 @@ __global__ void __launch_bounds__(512, 2) spmm_sell_kernel(polar_graph g, int ld
 #pragma unroll
     for (int v = 0; v < CPL; ++v) yv[v] = (T)fma((A)dg, (A)xi[v], -acc[v]);
     vstore_hint<T, CPL>(Y + (size_t)row * ldy + rg.col, yv, hp.stream);
-  });
+  };
+  if constexpr (POLAR_SELL_ASYNC != 0 && (CPL * sizeof(T)) % 16 == 0) {
+    extern __shared__ __align__(16) unsigned char sell_ring[];
+    sell_slice_pass_async<T, CPL, A>(g, rg, wid, nw, X, ldx, true, hp,
+                                     sell_ring + (size_t)warp * POLAR_SELL_STAGES * POLAR_SELL_BYTES * 32, row_end);
+  } else {
+    sell_slice_pass<T, CPL, A>(g, rg, wid, nw, X, ldx, true, hp, row_end);
+  }
 }
 
 template <typename T, int CPL>
@@ -128,14 +135,21 @@ static int launch_spmm_sell(const polar_graph& g, int ld, double shift, const vo
                             void* scratch, int precision, cudaStream_t st) {
   double* part = reinterpret_cast<double*>(scratch);
   int* hcount = reinterpret_cast<int*>(reinterpret_cast<char*>(scratch) + spmm_counter_offset(&g, precision));
+  // the async slice pass's ring (16 warps of 512 threads), when built in
+  const size_t ring = (POLAR_SELL_ASYNC != 0 && (CPL * sizeof(T)) % 16 == 0)
+                          ? (size_t)16 * POLAR_SELL_STAGES * POLAR_SELL_BYTES * 32 : 0;
+  static bool attr = false;
+  if (!attr && ring > 0)
+    cudaFuncSetAttribute(spmm_sell_kernel<T, CPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring);
+  attr = true;
   int dev = 0, sms = 0, nb = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, spmm_sell_kernel<T, CPL>, 512, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, spmm_sell_kernel<T, CPL>, 512, ring);
   if (nb < 1) nb = 1;
   const long long hot = (long long)(l2_hot_bytes_setting() / ((size_t)ld * sizeof(T)));
-  spmm_sell_kernel<T, CPL><<<nb * sms, 512, 0, st>>>(g, ld, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount,
-                                                      l2_mode_setting(), (int)(hot < g.n ? hot : g.n));
+  spmm_sell_kernel<T, CPL><<<nb * sms, 512, ring, st>>>(g, ld, shift, (const T*)X, ldx, (T*)Y, ldy, part, hcount,
+                                                         l2_mode_setting(), (int)(hot < g.n ? hot : g.n));
   count_launch();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_cuda_error("spmm launch", e);
