@@ -654,21 +654,22 @@ def run_solve(a):
         _lib.check(lib.polar_set_l2_policy(0, 64 << 20), "l2 policy")
         # heavy-row threshold of the shortlist width (mixed): rows above it go to warp chunks
         from polar_b200 import autotune
-        thr = {}
-        for t in (16, 32, 64, 128):
-            autotune.record(G, "mixed", R, (0, 1, t))
-            lib.polar_set_kernel_timing(1)
-            try:
-                S.msolve(op, Wd, tau, small[0], c["tol"], maxit=48, track=False, precision="mixed",
-                         active_pos=small[1])
-            except _lib.PolarError as e:
-                if e.status != _lib.POLAR_ERR_ITER_CAP:
-                    raise
-            kt = _lib.kernel_timing()
-            lib.polar_set_kernel_timing(0)
-            thr[t] = round(kt["spmm"][1] / max(1, kt["spmm"][0]), 4)
-        autotune.clear(G)
-        out["heavy_thresh_mixed_R%d" % R] = thr
+        for prec, Wm in (("mixed", Wd), ("fp64", Wd), ("mixed", W8)):
+            thr = {}
+            for t in (32, 64, 128, 256, 512, 1024):
+                autotune.record(G, prec, Wm.shape[1], (0, 1, t))
+                lib.polar_set_kernel_timing(1)
+                try:
+                    S.msolve(op, Wm, tau, small[0], c["tol"], maxit=48, track=False, precision=prec,
+                             active_pos=small[1])
+                except _lib.PolarError as e:
+                    if e.status != _lib.POLAR_ERR_ITER_CAP:
+                        raise
+                kt = _lib.kernel_timing()
+                lib.polar_set_kernel_timing(0)
+                thr[t] = round(kt["spmm"][1] / max(1, kt["spmm"][0]), 4)
+            autotune.clear(G)
+            out["heavy_thresh_%s_R%d" % (prec, Wm.shape[1])] = thr
         print(json.dumps({"workload": a.config, "quick": True, "n": n, "nnz": G.nnz,
                           "ms_per_launch_by_l2_policy": out}), flush=True)
         return
@@ -766,6 +767,10 @@ def run_diff(a):
     ts, oms = relaxed_rule(Gs, c["s"], K=c["K"])
     gs = relaxed_gradient(Gs, cs, ws, c["s"], tau=ts, om=oms, tol=1e-12)
     d = O.relaxed_dense(ns, Es, c["sigma"], cs, ws, c["s"], ts, oms)
+    # the same check with a fine composite rule (eps = 1e-9): the adjoint converges to the
+    # exact gradient as the rule does
+    tf, omf = relaxed_rule(Gs, c["s"], K=None, eps=1e-9)
+    gsf = relaxed_gradient(Gs, cs, ws, c["s"], tau=tf, om=omf, tol=1e-12)
     line = {"metric": "relaxed-weight objective and adjoint (FracTrace halves)", "unit": "s",
             "value": out["fp64"]["gradient_s"], "higher_is_better": False, "n_gpus": 1,
             "config": {"workload": a.config, "n": n, "m": int(len(E)), "candidates": len(cand), "K": c["K"],
@@ -776,7 +781,10 @@ def run_diff(a):
             "central_differences": fd, "max_rel_err_vs_central_differences": max(x["rel_err"] for x in fd),
             "dense_subgraph": {"n": ns, "m": int(len(Es)), "candidates": len(cs),
                                "max_rel_err_vs_rule": float(np.max(np.abs(gs - d["grad_q"]) / np.abs(d["grad_q"]))),
-                               "max_rel_err_vs_exact": float(np.max(np.abs(gs - d["grad"]) / np.abs(d["grad"])))}}
+                               "max_rel_err_vs_exact": float(np.max(np.abs(gs - d["grad"]) / np.abs(d["grad"]))),
+                               "fine_rule_poles": int(len(tf)),
+                               "fine_rule_max_rel_err_vs_exact":
+                                   float(np.max(np.abs(gsf - d["grad"]) / np.abs(d["grad"])))}}
     print(json.dumps(line), flush=True)
 
 

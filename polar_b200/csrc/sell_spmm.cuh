@@ -37,11 +37,10 @@
 namespace polar {
 
 // 16-byte asynchronous copy global -> shared (L2 only); src_bytes 0 fills zeros and reads
-// nothing.
-POLAR_D void cp_async16(void* smem, const void* gmem, int src_bytes, uint64_t pol) {
+// nothing.  The zero-fill form carries no L2 cache-policy operand.
+POLAR_D void cp_async16(void* smem, const void* gmem, int src_bytes) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;"
-               ::"r"(s), "l"(gmem), "r"(src_bytes), "l"(pol) : "memory");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
 }
 POLAR_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -270,8 +269,7 @@ POLAR_D void sell_slice_pass_async(const polar_graph& g, const RowGroup& rg, int
       const T* src = ok ? X + (size_t)jj[u] * ldx + rg.col : X;
 #pragma unroll
       for (int c = 0; c < NC; ++c)
-        cp_async16(slot(stage, u, c), reinterpret_cast<const unsigned char*>(src) + 16 * c, ok ? 16 : 0,
-                   ok ? hp.row(jj[u]) : hp.stream);
+        cp_async16(slot(stage, u, c), reinterpret_cast<const unsigned char*>(src) + 16 * c, ok ? 16 : 0);
     }
     cp_async_commit();
   };
