@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--solve", action="store_true", help="one shortlist solve with its kernel table")
     ap.add_argument("--quick", action="store_true", help="--solve: 48-iteration solves (an ncu-sized case)")
     ap.add_argument("--cache", default=None, help="directory for generated workloads (.npz, reused when present)")
+    ap.add_argument("--dense-only", action="store_true", help="diff-n1.13M: only the dense subgraph checks")
     return ap.parse_args()
 
 
@@ -748,16 +749,29 @@ def run_diff(a):
         return out, time.perf_counter() - t0
 
     out = {}
-    for prec in ("fp64", "mixed"):
-        grad, tg = timed(lambda: relaxed_gradient(G, cand, w, c["s"], tau=tau, om=om, tol=tol, precision=prec))
-        out[prec] = {"gradient_s": tg, "grad": grad}
-    (f, f_next), tf = timed(lambda: relaxed_objective(G, cand, w, c["s"], tau=tau, om=om, tol=tol, with_next=True))
-    g64 = out["fp64"]["grad"]
-    sample = [int(i) for i in rng.choice(np.flatnonzero(w >= 1e-3), 8, replace=False)]
-    fd = []
-    for i in sample:
-        v, t = timed(lambda: relaxed_central_difference(G, cand, w, c["s"], i, 1e-4, tau=tau, om=om, tol=tol))
-        fd.append({"i": i, "fd": v, "grad": float(g64[i]), "rel_err": abs(v - g64[i]) / abs(v), "seconds": t})
+    line = {"metric": "relaxed-weight objective and adjoint (FracTrace halves)", "unit": "s", "higher_is_better": False,
+            "n_gpus": 1,
+            "config": {"workload": a.config, "n": n, "m": int(len(E)), "candidates": len(cand), "K": c["K"],
+                       "s": c["s"], "sigma": c["sigma"], "tol": tol}}
+    if not a.dense_only:
+        for prec in ("fp64", "mixed"):
+            grad, tg = timed(lambda: relaxed_gradient(G, cand, w, c["s"], tau=tau, om=om, tol=tol, precision=prec))
+            out[prec] = {"gradient_s": tg, "grad": grad}
+        (f, f_next), tf = timed(lambda: relaxed_objective(G, cand, w, c["s"], tau=tau, om=om, tol=tol,
+                                                          with_next=True))
+        g64 = out["fp64"]["grad"]
+        sample = [int(i) for i in rng.choice(np.flatnonzero(w >= 1e-3), 8, replace=False)]
+        fd = []
+        for i in sample:
+            v, t = timed(lambda: relaxed_central_difference(G, cand, w, c["s"], i, 1e-4, tau=tau, om=om, tol=tol))
+            fd.append({"i": i, "fd": float(v), "grad": float(g64[i]), "rel_err": float(abs(v - g64[i]) / abs(v)),
+                       "seconds": t})
+        line.update({"value": out["fp64"]["gradient_s"], "forward_s": tf, "f": float(f),
+                     "dsigma": float(-c["s"] * f_next),
+                     "gradient_fp64_s": out["fp64"]["gradient_s"], "gradient_mixed_s": out["mixed"]["gradient_s"],
+                     "mixed_vs_fp64_max_rel": float(np.max(np.abs(out["mixed"]["grad"] - g64) / np.abs(g64))),
+                     "central_differences": fd,
+                     "max_rel_err_vs_central_differences": max(x["rel_err"] for x in fd)})
     # dense check: induced subgraph on the 3,000 lowest ids (the hubs and their mutual edges)
     ns = 3000
     Es = E[(E[:, 0] < ns) & (E[:, 1] < ns)]
@@ -769,22 +783,14 @@ def run_diff(a):
     d = O.relaxed_dense(ns, Es, c["sigma"], cs, ws, c["s"], ts, oms)
     # the same check with a fine composite rule (eps = 1e-9): the adjoint converges to the
     # exact gradient as the rule does
-    tf, omf = relaxed_rule(Gs, c["s"], K=None, eps=1e-9)
-    gsf = relaxed_gradient(Gs, cs, ws, c["s"], tau=tf, om=omf, tol=1e-12)
-    line = {"metric": "relaxed-weight objective and adjoint (FracTrace halves)", "unit": "s",
-            "value": out["fp64"]["gradient_s"], "higher_is_better": False, "n_gpus": 1,
-            "config": {"workload": a.config, "n": n, "m": int(len(E)), "candidates": len(cand), "K": c["K"],
-                       "s": c["s"], "sigma": c["sigma"], "tol": tol},
-            "forward_s": tf, "f": f, "dsigma": -c["s"] * f_next,
-            "gradient_fp64_s": out["fp64"]["gradient_s"], "gradient_mixed_s": out["mixed"]["gradient_s"],
-            "mixed_vs_fp64_max_rel": float(np.max(np.abs(out["mixed"]["grad"] - g64) / np.abs(g64))),
-            "central_differences": fd, "max_rel_err_vs_central_differences": max(x["rel_err"] for x in fd),
-            "dense_subgraph": {"n": ns, "m": int(len(Es)), "candidates": len(cs),
-                               "max_rel_err_vs_rule": float(np.max(np.abs(gs - d["grad_q"]) / np.abs(d["grad_q"]))),
-                               "max_rel_err_vs_exact": float(np.max(np.abs(gs - d["grad"]) / np.abs(d["grad"]))),
-                               "fine_rule_poles": int(len(tf)),
-                               "fine_rule_max_rel_err_vs_exact":
-                                   float(np.max(np.abs(gsf - d["grad"]) / np.abs(d["grad"])))}}
+    t_fine, om_fine = relaxed_rule(Gs, c["s"], K=None, eps=1e-9)
+    gsf = relaxed_gradient(Gs, cs, ws, c["s"], tau=t_fine, om=om_fine, tol=1e-12)
+    line["dense_subgraph"] = {
+        "n": ns, "m": int(len(Es)), "candidates": len(cs),
+        "max_rel_err_vs_rule": float(np.max(np.abs(gs - d["grad_q"]) / np.abs(d["grad_q"]))),
+        "max_rel_err_vs_exact": float(np.max(np.abs(gs - d["grad"]) / np.abs(d["grad"]))),
+        "fine_rule_poles": int(len(t_fine)),
+        "fine_rule_max_rel_err_vs_exact": float(np.max(np.abs(gsf - d["grad"]) / np.abs(d["grad"])))}
     print(json.dumps(line), flush=True)
 
 

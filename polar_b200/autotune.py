@@ -8,8 +8,8 @@ warp per row, 32 columns per pass).  Here the multi-shift CG's SpMM has three kn
   row of R columns takes R * elem / bytes lanes and a warp holds 32 / lanes rows;
 * the sliced-ELL copy of the light rows (on: warps read the neighbour lists of their rows
   slice-wise; off: CSR row loop);
-* the heavy-row threshold, as a multiple of the lanes per row: rows above it are cut into
-  chunks of at most 256 neighbours, one warp each.
+* the heavy-row threshold, as a multiple (4, 8, 16, 32 or 128) of the lanes per row: rows
+  above it are cut into chunks of at most 256 neighbours, one warp each.
 
 tune_msolve times `iters` iterations of the real solver (kernel-per-phase driver, CUDA
 graph blocks) for every combination and records the fastest; msolve then applies the
@@ -27,7 +27,7 @@ from . import solver as _solver
 __all__ = ["tune_msolve", "tuned", "record", "clear"]
 
 LANE_BYTES = (16, 32, 64)
-HEAVY_MULT = (4, 8, 16, 32)
+HEAVY_MULT = (4, 8, 16, 32, 128)
 
 
 def _ld(prec, R):
