@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(kBlock, POLAR_SPMM_MINB) mk_spmm(const __grid_
     for (int c = lane; c < ld; c += 32) wred[c] = 0.0;
     __syncwarp();
   }
-  const GatherHints hp = make_gather_hints(P.l2_mode, P.hot_rows);
+  const GatherHints hp = make_gather_hints(P.l2_mode, P.hot_rows, P.d, (size_t)ld * sizeof(T), P.n);
   const int wid = blockIdx.x * kWarps + warp;
   const int nw = gridDim.x * kWarps;
   if (MODE == 1 || MODE == 3) {

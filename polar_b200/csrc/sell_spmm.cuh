@@ -46,23 +46,67 @@ POLAR_D void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memo
 template <int N>
 POLAR_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+#ifndef POLAR_RANGE_POLICY
+#define POLAR_RANGE_POLICY 0  // 1: one address-range policy for all gathers (no per-gather choice)
+#endif
+#ifndef POLAR_SELL_DEG_INDPTR
+#define POLAR_SELL_DEG_INDPTR 0  // 1: a slice row's degree from indptr, not counted per neighbour
+#endif
+
 // L2 policies of one pass: rows below hot_rows are the most gathered rows of a
 // degree-ordered graph (kept with evict_last), the rest `cold`; `stream` for data read or
-// written once.
+// written once.  With POLAR_RANGE_POLICY the gather policy is one address-range policy over
+// the gathered block (evict_last on its first hot_rows rows, the secondary priority on the
+// rest), so a gather needs no choice between policies.
 struct GatherHints {
   uint64_t hot, cold, stream;
   int hot_rows;
-  POLAR_D uint64_t row(long long i) const { return i < hot_rows ? hot : cold; }
+  POLAR_D uint64_t row(long long i) const {
+#if POLAR_RANGE_POLICY
+    (void)i;
+    return hot;
+#else
+    return i < hot_rows ? hot : cold;
+#endif
+  }
 };
 
+// Range policy over [base, base + total): primary evict_last on the first `primary` bytes,
+// secondary evict_first (or unchanged) on the rest.  Sizes are 32-bit; blocks of 4 GB or
+// more fall back to the fractional policy.
+POLAR_D uint64_t l2_range_policy(const void* base, size_t primary, size_t total, bool cold_first) {
+  uint64_t p;
+  const unsigned ps = (unsigned)primary, ts = (unsigned)total;
+  if (cold_first)
+    asm volatile("createpolicy.range.global.L2::evict_last.L2::evict_first.b64 %0, [%1], %2, %3;"
+                 : "=l"(p) : "l"(base), "r"(ps), "r"(ts));
+  else
+    asm volatile("createpolicy.range.global.L2::evict_last.L2::evict_unchanged.b64 %0, [%1], %2, %3;"
+                 : "=l"(p) : "l"(base), "r"(ps), "r"(ts));
+  return p;
+}
+
 // mode 0: no hints (evict_normal everywhere); 1: hot rows evict_last, streams evict_first;
-// 2: as 1 with cold gathers evict_first.
-POLAR_D GatherHints make_gather_hints(int mode, int hot_rows) {
+// 2: as 1 with cold gathers evict_first.  `X`, `row_bytes`, `n`: the gathered block (used
+// by the range form).
+POLAR_D GatherHints make_gather_hints(int mode, int hot_rows, const void* X = nullptr, size_t row_bytes = 0,
+                                      long long n = 0) {
   GatherHints h;
   h.hot = l2_policy(mode ? 1 : 0);
   h.cold = l2_policy(mode == 2 ? 2 : 0);
   h.stream = l2_policy(mode ? 2 : 0);
   h.hot_rows = hot_rows;
+#if POLAR_RANGE_POLICY
+  const size_t total = row_bytes * (size_t)n;
+  if (mode && X && total > 0 && total < (size_t(1) << 32))
+    h.hot = l2_range_policy(X, row_bytes * (size_t)hot_rows, total, mode == 2);
+  else
+    h.hot = h.cold;
+#else
+  (void)X;
+  (void)row_bytes;
+  (void)n;
+#endif
   return h;
 }
 
@@ -198,7 +242,11 @@ POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, 
     A acc[CPL];
 #pragma unroll
     for (int v = 0; v < CPL; ++v) acc[v] = A(0);
+#if POLAR_SELL_DEG_INDPTR
+    const int deg = row >= 0 ? __ldg(g.d_indptr + row + 1) - __ldg(g.d_indptr + row) : 0;
+#else
     int deg = 0;
+#endif
     for (int k = 0; k < w; k += U) {
       T xv[U][CPL];
 #pragma unroll
@@ -215,7 +263,9 @@ POLAR_D void sell_slice_pass(const polar_graph& g, const RowGroup& rg, int wid, 
 #pragma unroll
       for (int u = 0; u < U; ++u)
         if (jj[u] >= 0) {
+#if !POLAR_SELL_DEG_INDPTR
           ++deg;
+#endif
           if (go)
 #pragma unroll
             for (int v = 0; v < CPL; ++v) acc[v] += (A)xv[u][v];

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(512, 2) spmm_sell_kernel(polar_graph g, int ld
   const int warp = threadIdx.x >> 5;
   const int wid = blockIdx.x * 16 + warp;
   const int nw = gridDim.x * 16;
-  const GatherHints hp = make_gather_hints(l2_mode, hot_rows);
+  const GatherHints hp = make_gather_hints(l2_mode, hot_rows, X, (size_t)ldx * sizeof(T), g.n);
   heavy_chunk_pass<T, CPL, false, A>(
       g, rg, wid, nw, X, ldx, ld, true, s_idx[warp], part, hcount, hp,
       [&](int i, int cnt, auto& acc, auto& xi) {
