@@ -308,6 +308,21 @@ int polar_maintain(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32, int p, in
                    const void* d_U, int u_f32, int ldu, const int32_t* d_win, const double* d_G,
                    const int32_t* d_es, int N, double* d_h, double* d_t, void* d_tmp,
                    polar_stream_t stream);
+/* Column-split maintenance (the q sketch columns spread over several GPUs, each holding
+ * its own columns of X, Y and G): the same X, Y update on this GPU's q columns, with this
+ * GPU's share of the cache change written to d_dh, d_dt ([p][N] FP64) instead of h, t:
+ *   dh = cc^2 |xi|^2 - 2 cc (w^X[a] - w^X[b]),  dt = cc^2 |eta|^2 + 2 cc (w^Y[a] - w^Y[b]),
+ * cc = (u[a] - u[b]) / D, norms and w over the local columns.  The shares summed over the
+ * GPUs (an all-reduce) enter the caches through polar_cache_apply:
+ *   h = max(0, h + dh), t = max(0, t + dt)   (count = p * N entries).
+ * The reference's maintenance (polar_gpu.py:242-249) is the one-GPU case; it has no
+ * column split. */
+int polar_maintain_split(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32, int p, int nA, int q,
+                         const void* d_U, int u_f32, int ldu, const int32_t* d_win, const double* d_G,
+                         const int32_t* d_es, int N, double* d_dh, double* d_dt, void* d_tmp,
+                         polar_stream_t stream);
+int polar_cache_apply(double* d_h, const double* d_dh, double* d_t, const double* d_dt, int64_t count,
+                      polar_stream_t stream);
 
 /* ---- F update (polar_gpu.py:250): with e = *sel, (a, b) = cand[e]:
  *      F[a] += G[e]; F[b] -= G[e]  (FP64 rows of q) ---- */

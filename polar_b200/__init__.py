@@ -6,7 +6,8 @@ true_marginals, degree_greedy, random_set, chunk_width.  The compute runs in the
 hand-written kernels of libpolar.so (include/polar.h) through ctypes; there is no CPU
 fallback.  Keyword-only extensions: precision='fp64'|'mixed', K=<fixed pole count>.
 Beyond the reference: FracTrace / relaxed_gradient / relaxed_objective, the relaxed-weight
-objective f_s(w, sigma) with its adjoint (polar_b200.adjoint).
+objective f_s(w, sigma) with its adjoint (polar_b200.adjoint); polar_split, the greedy with
+its sketch and shortlist columns split over the ranks of a process group (polar_b200.split).
 """
 from .quadrature import composite, fixed_rule, poles
 from .sketch import sketches, chunk_width
@@ -15,7 +16,7 @@ from .synth import chung_lu, candidates
 __version__ = "0.1.0"
 
 _DEVICE_NAMES = ("Graph", "Op", "msolve", "Counter", "polar", "Greedy", "true_marginals", "degree_greedy", "random_set",
-                 "FracTrace", "relaxed_gradient", "relaxed_objective")
+                 "FracTrace", "relaxed_gradient", "relaxed_objective", "polar_split")
 
 
 def __getattr__(name):
@@ -30,6 +31,9 @@ def __getattr__(name):
     if name in ("polar", "Greedy", "true_marginals", "degree_greedy", "random_set"):
         from . import greedy
         return getattr(greedy, name)
+    if name == "polar_split":
+        from . import split
+        return split.polar_split
     if name in ("FracTrace", "relaxed_gradient", "relaxed_objective"):
         from . import adjoint
         return getattr(adjoint, name)

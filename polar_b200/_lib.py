@@ -114,6 +114,8 @@ SIGNATURES = {
     "polar_select": (_I, [_P, _P, _P, _P, _P, _P]),
     "polar_maintain_tmp_bytes": (_S, [_I, _I, _I]),
     "polar_maintain": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _I, _P, _P, _P, _P]),
+    "polar_maintain_split": (_I, [_P, _I, _P, _I, _I, _I, _I, _I, _P, _I, _I, _P, _P, _P, _I, _P, _P, _P, _P]),
+    "polar_cache_apply": (_I, [_P, _P, _P, _P, _I64, _P]),
     "polar_rank1_rows": (_I, [_P, _I, _I, _P, _P, _P, _P]),
 }
 

@@ -364,6 +364,31 @@ __global__ void maint_cache_kernel(int p, int nA, int N, const void* U, int u_f3
   t[o] = fmax(0.0, t[o] + 2.0 * cc * dy + cc * cc * m.neta[j]);
 }
 
+// Column-split form (the sketch columns spread over several ranks): this rank's share of
+// the cache change, summed over the ranks before cache_apply_kernel clamps it in.
+__global__ void maint_delta_kernel(int p, int nA, int N, const void* U, int u_f32, int ldu, const int32_t* win,
+                                   const int32_t* es, MaintTmp m, double* dh, double* dt) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)p * N) return;
+  const int j = (int)(g / N), e = (int)(g % N);
+  const int uc = win[0];
+  const int a = es[2 * e], b = es[2 * e + 1];
+  const double cc = (ldv(U, u_f32, ((size_t)j * nA + a) * ldu + uc) - ldv(U, u_f32, ((size_t)j * nA + b) * ldu + uc)) /
+                    m.D[j];
+  const double dx = m.wX[(size_t)j * nA + a] - m.wX[(size_t)j * nA + b];
+  const double dy = m.wY[(size_t)j * nA + a] - m.wY[(size_t)j * nA + b];
+  const size_t o = (size_t)j * N + e;
+  dh[o] = cc * cc * m.nxi[j] - 2.0 * cc * dx;
+  dt[o] = cc * cc * m.neta[j] + 2.0 * cc * dy;
+}
+
+__global__ void cache_apply_kernel(double* h, const double* dh, double* t, const double* dt, long long count) {
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < count; o += (long long)gridDim.x * blockDim.x) {
+    h[o] = fmax(0.0, h[o] + dh[o]);
+    t[o] = fmax(0.0, t[o] + dt[o]);
+  }
+}
+
 // Winner record: win[0] = shortlist position, win[1] = aa, win[2] = bb, win[4..5] = e.
 __global__ void select_kernel(const int64_t* shortl, const int32_t* best, const int32_t* es, uint8_t* live,
                               int32_t* win) {
@@ -492,9 +517,11 @@ extern "C" int polar_select(const int64_t* d_short, const int32_t* d_best, const
   return check_launch("select");
 }
 
-extern "C" int polar_maintain(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32, int p, int nA, int q, const void* d_U,
-                              int u_f32, int ldu, const int32_t* d_win, const double* d_G, const int32_t* d_es, int N,
-                              double* d_h, double* d_t, void* d_tmp, polar_stream_t stream) {
+// Both maintenance forms: delta == false updates h, t in place; delta == true writes this
+// rank's cache change to h, t (as dh, dt).
+static int maintain(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32, int p, int nA, int q, const void* d_U,
+                    int u_f32, int ldu, const int32_t* d_win, const double* d_G, const int32_t* d_es, int N,
+                    double* d_h, double* d_t, void* d_tmp, polar_stream_t stream, bool delta) {
   clear_error();
   if (!d_X || !d_Y || !d_U || !d_win || !d_G || !d_es || !d_h || !d_t || !d_tmp || p < 1 || nA < 1 || q < 1 ||
       ldx < q || ldy < q)
@@ -526,10 +553,39 @@ extern "C" int polar_maintain(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32
   if (rc) return rc;
   if (N > 0) {
     const long long t2 = (long long)p * N;
-    maint_cache_kernel<<<(int)((t2 + 255) / 256), 256, 0, st>>>(p, nA, N, d_U, u_f32, ldu, d_win, d_es, m, d_h, d_t);
-    rc = check_launch("maint_cache");
+    if (delta)
+      maint_delta_kernel<<<(int)((t2 + 255) / 256), 256, 0, st>>>(p, nA, N, d_U, u_f32, ldu, d_win, d_es, m, d_h, d_t);
+    else
+      maint_cache_kernel<<<(int)((t2 + 255) / 256), 256, 0, st>>>(p, nA, N, d_U, u_f32, ldu, d_win, d_es, m, d_h, d_t);
+    rc = check_launch(delta ? "maint_delta" : "maint_cache");
   }
   return rc;
+}
+
+extern "C" int polar_maintain(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32, int p, int nA, int q, const void* d_U,
+                              int u_f32, int ldu, const int32_t* d_win, const double* d_G, const int32_t* d_es, int N,
+                              double* d_h, double* d_t, void* d_tmp, polar_stream_t stream) {
+  return maintain(d_X, ldx, d_Y, ldy, xy_f32, p, nA, q, d_U, u_f32, ldu, d_win, d_G, d_es, N, d_h, d_t, d_tmp, stream,
+                  false);
+}
+
+extern "C" int polar_maintain_split(void* d_X, int ldx, void* d_Y, int ldy, int xy_f32, int p, int nA, int q,
+                                    const void* d_U, int u_f32, int ldu, const int32_t* d_win, const double* d_G,
+                                    const int32_t* d_es, int N, double* d_dh, double* d_dt, void* d_tmp,
+                                    polar_stream_t stream) {
+  return maintain(d_X, ldx, d_Y, ldy, xy_f32, p, nA, q, d_U, u_f32, ldu, d_win, d_G, d_es, N, d_dh, d_dt, d_tmp,
+                  stream, true);
+}
+
+extern "C" int polar_cache_apply(double* d_h, const double* d_dh, double* d_t, const double* d_dt, int64_t count,
+                                 polar_stream_t stream) {
+  clear_error();
+  if (!d_h || !d_dh || !d_t || !d_dt || count < 0) return set_error(POLAR_ERR_BAD_ARG, "bad arguments");
+  if (count == 0) return POLAR_OK;
+  const long long blocks = (count + 255) / 256;
+  cache_apply_kernel<<<(int)(blocks < 148 * 16 ? blocks : 148 * 16), 256, 0, (cudaStream_t)stream>>>(d_h, d_dh, d_t,
+                                                                                                     d_dt, count);
+  return check_launch("cache_apply");
 }
 
 extern "C" int polar_rank1_rows(double* d_F, int ldf, int q, const double* d_G, const int64_t* d_cand,
