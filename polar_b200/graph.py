@@ -16,7 +16,7 @@ import torch
 
 from . import _lib
 
-__all__ = ["Graph", "Op", "default_device"]
+__all__ = ["Graph", "Op", "default_device", "csr_from_edges", "sell_slices", "sell_slices_torch"]
 
 
 def default_device():
@@ -63,6 +63,56 @@ def sell_slices(indptr, indices, light_mask, S, window=4096):
     if off[-1] >= 2 ** 31:
         raise ValueError("sliced ELL too large for int32 offsets")
     return off.astype(np.int32), rows_p.ravel().astype(np.int32), sidx.astype(np.int32)
+
+
+def csr_from_edges(n, u, v):
+    """Symmetric unweighted adjacency CSR from an edge list, with torch on the edge arrays'
+    device (the ingestion step of realworld/graphs.py:46-58 and polar_gpu.py:48-58, which
+    build it with scipy on the host): both directions, sorted by (row, column), repeated
+    pairs merged.  Returns (indptr int32[n+1], indices int32[nnz], counts int64[nnz]); a
+    count above 1 is a merged repeated edge (a weight above 1)."""
+    n = int(n)
+    rows = torch.cat([u, v]).to(torch.int64)
+    cols = torch.cat([v, u]).to(torch.int64)
+    key, _ = torch.sort(rows * n + cols)
+    uniq, counts = torch.unique_consecutive(key, return_counts=True)
+    r = torch.div(uniq, n, rounding_mode="floor")
+    indptr = torch.zeros(n + 1, dtype=torch.int64, device=u.device)
+    indptr[1:] = torch.cumsum(torch.bincount(r, minlength=n), 0)
+    return indptr.to(torch.int32), (uniq - r * n).to(torch.int32), counts
+
+
+def sell_slices_torch(indptr, indices, light_mask, S, window=4096):
+    """sell_slices with torch on the arrays' device; the same three arrays (as int32
+    tensors on that device)."""
+    dev = indptr.device
+    rows = torch.nonzero(light_mask).flatten()
+    if rows.numel() == 0:
+        z = torch.zeros(1, dtype=torch.int32, device=dev)
+        return z, torch.zeros(0, dtype=torch.int32, device=dev), torch.zeros(0, dtype=torch.int32, device=dev)
+    ip = indptr.to(torch.int64)
+    deg = ip[rows + 1] - ip[rows]
+    dmax = int(deg.max())
+    win = torch.arange(rows.numel(), device=dev) // window
+    _, order = torch.sort(win * (dmax + 1) + (dmax - deg), stable=True)
+    rows = rows[order]
+    deg = deg[order]
+    ns = -(-rows.numel() // S)
+    pad = ns * S - rows.numel()
+    rows_p = torch.cat([rows, torch.full((pad,), -1, dtype=torch.int64, device=dev)])
+    deg_p = torch.cat([deg, torch.zeros(pad, dtype=torch.int64, device=dev)])
+    width = deg_p.view(ns, S).max(dim=1).values
+    off = torch.zeros(ns + 1, dtype=torch.int64, device=dev)
+    off[1:] = torch.cumsum(width * S, 0)
+    sidx = torch.full((int(off[-1]),), -1, dtype=torch.int32, device=dev)
+    rr = torch.repeat_interleave(torch.arange(ns * S, device=dev), deg_p)
+    start = torch.cumsum(deg_p, 0) - deg_p
+    k_in = torch.arange(rr.numel(), device=dev) - torch.repeat_interleave(start, deg_p)
+    src = torch.repeat_interleave(ip[rows_p.clamp_min(0)], deg_p) + k_in
+    sidx[off[rr // S] + k_in * S + rr % S] = indices[src].to(torch.int32)
+    if int(off[-1]) >= 2 ** 31:
+        raise ValueError("sliced ELL too large for int32 offsets")
+    return off.to(torch.int32), rows_p.to(torch.int32), sidx
 
 
 def row_blocks(indptr, heavy_thresh, row_cost=4, target=None):
@@ -133,25 +183,38 @@ class Graph:
         if len(w) != len(u):
             raise ValueError("weights must match edges")
         deg = np.bincount(u, w, self.n) + np.bincount(v, w, self.n)
-        A = sp.csr_matrix((np.r_[w, w], (np.r_[u, v], np.r_[v, u])), shape=(self.n, self.n))
-        A.sum_duplicates()
-        A.sort_indices()
-        if A.nnz >= 2 ** 31:
-            raise ValueError("graph too large for int32 CSR")
         self.dmax = float(deg.max()) if self.n else 0.0
         self.m = len(u)
         self.edges = edges
         self.weights = w
         self.M0 = _HostM0(self)
-        self._indptr_h = A.indptr.astype(np.int32)
-        self._indices_h = A.indices.astype(np.int32)
-        self._data_h = A.data
         self._deg_h = deg
-        self.nnz = int(A.nnz)
-        self.weighted = weights is not None and not np.all(self._data_h == 1.0)
         dev = self.device
-        self.indptr = _i32(self._indptr_h, dev)
-        self.indices = _i32(self._indices_h, dev)
+        self._ind_h = self._dat_h = None
+        csr = None
+        if weights is None and dev.type == "cuda" and 0 < 2 * len(u) < 2 ** 31:
+            # ingestion on the device; repeated edges (merged weights) take the host path
+            csr = csr_from_edges(self.n, torch.as_tensor(u).to(dev), torch.as_tensor(v).to(dev))
+            if bool((csr[2] > 1).any()):
+                csr = None
+        if csr is not None:
+            self.indptr, self.indices = csr[0], csr[1]
+            self._indptr_h = self.indptr.cpu().numpy()
+            self.nnz = int(self.indices.numel())
+            self.weighted = False
+        else:
+            A = sp.csr_matrix((np.r_[w, w], (np.r_[u, v], np.r_[v, u])), shape=(self.n, self.n))
+            A.sum_duplicates()
+            A.sort_indices()
+            if A.nnz >= 2 ** 31:
+                raise ValueError("graph too large for int32 CSR")
+            self._indptr_h = A.indptr.astype(np.int32)
+            self._ind_h = A.indices.astype(np.int32)
+            self._dat_h = A.data
+            self.nnz = int(A.nnz)
+            self.weighted = weights is not None and not np.all(self._dat_h == 1.0)
+            self.indptr = _i32(self._indptr_h, dev)
+            self.indices = _i32(self._ind_h, dev)
         if self.weighted:
             self.wts = torch.as_tensor(self._data_h, dtype=torch.float64).to(dev)
             self.diag = torch.as_tensor(deg + self.sigma, dtype=torch.float64).to(dev)
@@ -159,6 +222,20 @@ class Graph:
             self.wts = None
             self.diag = None
         self._split_heavy(int(heavy_thresh))
+
+    @property
+    def _indices_h(self):
+        """Host copy of the neighbour indices (read back once when built on the device)."""
+        if self._ind_h is None:
+            self._ind_h = self.indices.cpu().numpy()
+        return self._ind_h
+
+    @property
+    def _data_h(self):
+        """Host CSR values (unit weights when built on the device)."""
+        if self._dat_h is None:
+            self._dat_h = np.ones(self.nnz)
+        return self._dat_h
 
     # -- heavy-row split ---------------------------------------------------------------
     CHUNK = 256  # neighbours per heavy-row chunk (one warp per chunk in the solver)
@@ -211,12 +288,19 @@ class Graph:
         if not hasattr(self, "_sell_cache"):
             self._sell_cache = {}
         if key not in self._sell_cache:
-            degs = np.diff(self._indptr_h.astype(np.int64))
-            off, rows, sidx = sell_slices(self._indptr_h, self._indices_h, degs <= thresh, S)
             dev = self.device
-            self._sell_cache[key] = dict(ns=len(off) - 1, off=_i32(off, dev),
-                                         rows=_i32(rows if len(rows) else np.zeros(1, np.int32), dev),
-                                         idx=_i32(sidx if len(sidx) else np.zeros(1, np.int32), dev))
+            if dev.type == "cuda":
+                ip = self.indptr.to(torch.int64)
+                off, rows, sidx = sell_slices_torch(self.indptr, self.indices, (ip[1:] - ip[:-1]) <= thresh, S)
+                one = torch.zeros(1, dtype=torch.int32, device=dev)
+                self._sell_cache[key] = dict(ns=off.numel() - 1, off=off, rows=rows if rows.numel() else one,
+                                             idx=sidx if sidx.numel() else one)
+            else:
+                degs = np.diff(self._indptr_h.astype(np.int64))
+                off, rows, sidx = sell_slices(self._indptr_h, self._indices_h, degs <= thresh, S)
+                self._sell_cache[key] = dict(ns=len(off) - 1, off=_i32(off, dev),
+                                             rows=_i32(rows if len(rows) else np.zeros(1, np.int32), dev),
+                                             idx=_i32(sidx if len(sidx) else np.zeros(1, np.int32), dev))
         return self._sell_cache[key]
 
     def struct(self, extra=None, heavy_thresh=None, sell_rows=0):

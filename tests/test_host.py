@@ -267,3 +267,30 @@ def test_candidates_batched_identity_and_cache(tmp_path):
     assert len(list(tmp_path.iterdir())) == 1
     np.testing.assert_array_equal(E1, E2)
     np.testing.assert_array_equal(c1, c2)
+
+
+def test_device_ingestion_matches_host_csr_and_slices():
+    """The torch ingestion (run here on CPU tensors; on the GPU for Graph on a CUDA device)
+    builds the scipy CSR and the sliced ELL of the host path exactly."""
+    import scipy.sparse as sp
+    import torch
+    from polar_b200.graph import csr_from_edges, sell_slices, sell_slices_torch
+    from polar_b200.synth import chung_lu
+    n = 5000
+    E = chung_lu(n, 8.0, 2.2, 5, min_degree=1)
+    u, v = E[:, 0], E[:, 1]
+    A = sp.csr_matrix((np.ones(2 * len(u)), (np.r_[u, v], np.r_[v, u])), shape=(n, n))
+    A.sum_duplicates()
+    A.sort_indices()
+    ip, ind, cnt = csr_from_edges(n, torch.as_tensor(u), torch.as_tensor(v))
+    assert np.array_equal(ip.numpy(), A.indptr) and np.array_equal(ind.numpy(), A.indices)
+    assert int(cnt.max()) == 1
+    deg = np.diff(A.indptr)
+    for thresh, S in ((32, 8), (512, 4), (10 ** 6, 16)):
+        ref = sell_slices(A.indptr.astype(np.int32), A.indices.astype(np.int32), deg <= thresh, S, window=512)
+        got = sell_slices_torch(ip, ind, torch.as_tensor(deg <= thresh), S, window=512)
+        for r, g in zip(ref, got):
+            assert np.array_equal(r, g.numpy())
+    # a repeated edge shows as a merged count of 2
+    _, _, cnt = csr_from_edges(4, torch.tensor([0, 1, 0]), torch.tensor([1, 2, 1]))
+    assert sorted(cnt.tolist()) == [1, 1, 2, 2]
