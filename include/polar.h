@@ -190,7 +190,7 @@ void polar_set_sell(int on);
 /* L2 eviction priorities of the solver's SpMM and direction update (default driver only):
  * mode 0 none; 1: the first hot_bytes / (row bytes) rows of the direction (the most
  * gathered rows of a degree-ordered graph) are gathered and stored with evict_last, the
- * neighbour indices and the SpMM output with evict_first; 2 (default, 64 MB): as 1, with
+ * neighbour indices and the SpMM output with evict_first; 2 (default, 32 MB): as 1, with
  * gathers of the other rows evict_first too.  Caching only: results are identical in
  * every mode. */
 int polar_set_l2_policy(int mode, size_t hot_bytes);

@@ -510,10 +510,11 @@ extern "C" int polar_set_mixed_residual(int bits) {
 }
 
 // L2 policy of the kernel-per-phase driver (SolvePrm::l2_mode / hot_rows).  Default mode 2
-// (hot 64 MB evict_last, other gathers and streams evict_first): 5-7 % faster SpMM launches
-// on the 4M-vertex graph at R = 16 and 128 in both precisions.
+// (hot 32 MB evict_last, other gathers and streams evict_first): 5-7 % faster SpMM launches
+// on the 4M-vertex graph at R = 16 and 128 in both precisions than no hints, and 1.5 %
+// faster at R = 16 than a 64 MB hot prefix.
 static int g_l2_mode = 2;
-static size_t g_l2_hot_bytes = size_t(64) << 20;
+static size_t g_l2_hot_bytes = size_t(32) << 20;
 
 namespace polar {
 int l2_mode_setting() { return g_l2_mode; }

@@ -35,7 +35,7 @@ def _rank_main(rank, world, port, out):
 
 
 def test_replicas_two_ranks_gloo():
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_rank_main, args=(2, _free_port(), out), nprocs=2, join=True)
     seeds = {out[r][0] for r in range(2)}

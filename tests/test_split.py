@@ -186,7 +186,7 @@ def test_shares_cover_the_range():
 
 def test_column_split_two_ranks_gloo():
     one = _run(Comm())
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_rank_main, args=(2, _free_port(), out), nprocs=2, join=True)
     for r in range(2):
