@@ -120,17 +120,37 @@ class Graph:
 class Op:
     """y = (M0 + sum_S b b^T + shift I) x (polar_gpu.py:63-80)."""
 
-    def __init__(self, G):
+    def __init__(self, G, threads=1):
         self.M0 = G.M0
         self.A = []
         self.B = []
+        # threads > 1: the product with M0 in row blocks on a thread pool (the sparse
+        # product releases the interpreter lock); each row is computed as with one thread
+        self.pool, self.rows = None, []
+        if threads > 1:
+            from concurrent.futures import ThreadPoolExecutor
+            n = self.M0.shape[0]
+            cuts = [(i * n) // (4 * threads) for i in range(4 * threads + 1)]
+            self.rows = [(lo, hi, self.M0[lo:hi]) for lo, hi in zip(cuts[:-1], cuts[1:]) if hi > lo]
+            self.pool = ThreadPoolExecutor(threads)
 
     def add(self, a, b):
         self.A.append(int(a))
         self.B.append(int(b))
 
+    def _m0(self, x):
+        if self.pool is None:
+            return self.M0 @ x
+        y = np.empty((self.M0.shape[0],) + x.shape[1:], dtype=np.result_type(self.M0.dtype, x.dtype))
+
+        def blk(r):
+            y[r[0]:r[1]] = r[2] @ x
+
+        list(self.pool.map(blk, self.rows))
+        return y
+
     def __call__(self, x, shift):
-        y = self.M0 @ x
+        y = self._m0(x)
         if shift:
             y = y + shift * x
         if self.A:
@@ -148,14 +168,16 @@ class Counter:
         self.rhs = 0
 
 
-def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, on_iteration=None):
+def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, on_iteration=None, threads=1):
     """Multi-shift CG for (M + tau_j I) U = W over all poles and columns
     (polar_gpu.py:88-133).
 
     Column c runs its own seed CG on the smallest pole tau[0]; pole j follows through
     the zeta recurrence, its iterate X and direction P are kept on the `active` rows
     only, and it freezes once |zeta| * ||r|| <= tol * ||w||.  With `track`, the three
-    scalars (h, ip, pn) give ||U_j[:, c]||^2 without full vectors.  Returns
+    scalars (h, ip, pn) give ||U_j[:, c]||^2 without full vectors.  threads > 1 spreads
+    the shifted updates of X and P (elementwise, the bulk of the work) over a thread pool
+    by (pole, row block); every element is computed as with one thread.  Returns
     (X[p, nA, R], h[p, R] or None, iterations[R])."""
     W = np.asarray(W, np.float64)
     n, R = W.shape
@@ -181,6 +203,13 @@ def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, on_
     bp = np.zeros(R)
     iters = np.zeros(R, dtype=np.int64)
     safe = lambda x: np.where(act, x, 1.0)
+    pool, blocks = None, []
+    if threads > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        nA = len(active)
+        per = max(1, (p * nA) // (4 * threads))
+        blocks = [(j, lo, min(nA, lo + per)) for j in range(p) for lo in range(0, nA, per)]
+        pool = ThreadPoolExecutor(threads)
     for it in range(maxit):
         v = op(d, float(tau[0]))
         dv = np.sum(d * v, axis=0)
@@ -194,8 +223,19 @@ def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, on_
         m = live & act[None]
         aj = np.where(m, a * fac, 0.0)
         bj = be * fac * fac
-        X += aj[:, None, :] * P
-        P = np.where(m[:, None, :], zn[:, None, :] * rn[active][None] + bj[:, None, :] * P, P)
+        if pool is None:
+            X += aj[:, None, :] * P
+            P = np.where(m[:, None, :], zn[:, None, :] * rn[active][None] + bj[:, None, :] * P, P)
+        else:
+            ra = rn[active]
+
+            def upd(blk, aj=aj, bj=bj, zn=zn, m=m, ra=ra):
+                j, lo, hi = blk
+                Xs, Ps = X[j, lo:hi], P[j, lo:hi]
+                Xs += aj[j] * Ps
+                Ps[...] = np.where(m[j], zn[j] * ra[lo:hi] + bj[j] * Ps, Ps)
+
+            list(pool.map(upd, blocks))
         if track:
             h += 2.0 * aj * ip + aj * aj * pn
             ip = np.where(m, bj * (ip + aj * pn), ip)
@@ -217,7 +257,11 @@ def msolve(op, W, tau, active, tol, maxit=100000, track=False, counter=None, on_
         if it % 8 == 7 and not act.any():
             break
     else:
+        if pool is not None:
+            pool.shutdown()
         raise RuntimeError("multi-shift CG iteration cap")
+    if pool is not None:
+        pool.shutdown()
     if counter is not None:
         counter.spmv += int(iters.sum())
         counter.rhs += R

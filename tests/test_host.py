@@ -294,3 +294,24 @@ def test_device_ingestion_matches_host_csr_and_slices():
     # a repeated edge shows as a merged count of 2
     _, _, cnt = csr_from_edges(4, torch.tensor([0, 1, 0]), torch.tensor([1, 2, 1]))
     assert sorted(cnt.tolist()) == [1, 1, 2, 2]
+
+
+def test_oracle_threads_give_identical_solves():
+    """The oracle's threaded sparse product and shifted updates (the bench's CPU legs use all
+    host threads) compute every element as the one-thread path does."""
+    from oracle import polar_oracle as O
+    from polar_b200.quadrature import poles
+    from polar_b200.synth import candidates, chung_lu
+    n = 3000
+    E = chung_lu(n, 6.0, 2.4, 2, min_degree=1)
+    cand = candidates(n, E, 2000, 5)
+    G = O.Graph(n, E, 1e-2)
+    tau, _, _ = poles("frac", 0.5, 1e-2, G.Lam(5), 1e-2, K=12)
+    act = np.unique(cand)
+    W = np.zeros((n, 6))
+    W[cand[:6, 0], np.arange(6)] = 1.0
+    W[cand[:6, 1], np.arange(6)] = -1.0
+    one = O.msolve(O.Op(G), W, tau, act, 1e-8, track=True)
+    many = O.msolve(O.Op(G, threads=4), W, tau, act, 1e-8, track=True, threads=4)
+    for a, b in zip(one, many):
+        assert np.array_equal(a, b)
