@@ -274,6 +274,8 @@ int polar_pair_norms(const void* d_X, int x_f32, int p, int nA, int ldx, int col
  *            adjoint d f_s / d w_e at w = 0, the candidate screen; no reference counterpart)
  * Dead candidates (live[e] == 0) score -inf.  The B best by (score desc, index asc) —
  * the order of a stable argsort of -score — go to out_idx / out_score (device).
+ * d_score_all (optional, N doubles) receives every candidate's score before the live
+ * mask, dead candidates included.
  * d_tmp: polar_topb_tmp_bytes(N, B) bytes. */
 size_t polar_topb_tmp_bytes(int N, int B);
 int polar_score_topb(const double* d_h, const double* d_t, const double* d_tau, const double* d_om,
