@@ -810,11 +810,12 @@ def run_diff(a):
 def run_reference(a):
     """The reference's algorithm on the host cores for the same workload and metric: the
     oracle (a NumPy FP64 restatement of realworld/polar_gpu.py, pinned to the reference's
-    own outputs; the reference itself needs CuPy and a GPU).  Each step is one timed
-    multi-shift CG iteration of the workload's shortlist solve (B columns, all K poles, all
-    active rows, full graph); value = s per iteration x the seed iterations of a round (the
-    FP64 GPU path's per-round counts, profiles/iterations_per_round.json) + the per-round
-    scoring and maintenance, timed once.  Rank 0 alone runs; other ranks exit."""
+    own outputs; the reference itself needs CuPy and a GPU).  Each timed step is
+    ceil(20 / K) multi-shift CG iterations of the workload's shortlist solve (B columns, all K
+    poles, all active rows, full graph), so that at least 20 real iterations are timed; each
+    warm-up step is one iteration.  value = s per iteration x the seed iterations of a round
+    (the FP64 GPU path's per-round counts, profiles/iterations_per_round.json) + the
+    per-round scoring and maintenance, timed once.  Rank 0 alone runs; other ranks exit."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -828,23 +829,26 @@ def run_reference(a):
     c = inp["cfg"]
     t0 = time.perf_counter()
     nth = host_threads()
-    parts = oracle_round_parts(inp, a.warmup + a.steps, warm=1 + a.warmup, threads=nth)
+    per_step = -(-20 // max(1, a.steps))
+    parts = oracle_round_parts(inp, per_step * a.steps, warm=1 + a.warmup, threads=nth)
     run_s = time.perf_counter() - t0
     per, greedy_s, it_s = cpu_round_estimate(parts, rec["fp64_per_round"], max(rec["fp64_bank"]), inp["k"], c["q"])
     cpu = {"value": per, "unit": UNIT, "cores": nth, "kind": "port", "greedy_s": greedy_s,
            "sample": (f"oracle multi-shift CG on the shortlist solve ({c['B']} columns, {parts['p']} poles, "
-                      f"{parts['nA']} active rows): {a.steps} timed iterations of {it_s:.2f} s x "
+                      f"{parts['nA']} active rows): {len(parts['iteration_s'])} timed iterations "
+                      f"({a.steps} steps of {per_step}), {it_s:.2f} s each, x "
                       f"{np.mean(rec['fp64_per_round']):.0f} seed iterations per round (FP64 GPU counts) + scoring "
                       f"{parts['score_s']:.2f} s + maintenance {parts['maintain_s']:.2f} s; sparse product and "
                       f"shifted updates on {nth} host threads, other NumPy work on one")}
     line = {"impl": "reference", "metric": METRIC, "value": per, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": it_s * 1e3, "higher_is_better": False, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": per_step * it_s * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Chung-Lu stand-in for the %s shape)" % (
                 "com-LiveJournal" if a.config == "full-n4M" else a.config),
             "config": {"workload": a.config, "n": inp["n"], "m": int(len(inp["E"])), "N": inp["N"], "K": c["K"],
                        "q": c["q"], "B": c["B"], "k": inp["k"], "s": c["s"], "sigma": c["sigma"], "tol": c["tol"],
-                       "step": "one multi-shift CG iteration of a round's shortlist solve (value: s/round)"},
+                       "step": "%d multi-shift CG iterations of a round's shortlist solve (value: s/round)"
+                               % per_step},
             "greedy_s": greedy_s, "timed_run_s": run_s,
             "cpu_baseline": cpu, "e2e": {"value": per, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
