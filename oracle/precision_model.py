@@ -12,6 +12,9 @@ Knobs (each True = stored in FP32):
   dm   the SpMM's copy of the direction   v    the SpMM output
   xp   the shifted iterates X, P (rounded once per M-step deferred update)
 The device's mixed scheme is r = d = False, dm = v = xp = True.
+ru = m adds reliable updates: the seed iterate x is kept on all rows in FP64 (x += alpha d
+with the direction the SpMM read), and every m iterations the recurred residual is replaced
+by the true residual W - (M + tau_0) x accumulated in FP64 (then stored as the r knob says).
 """
 import numpy as np
 import scipy.sparse as sp
@@ -33,8 +36,9 @@ def laplacian(n, edges):
 
 
 def shortlist_solve(A, deg, sigma, tau, om, pairs, tol=1e-7, M=16, r=False, d=False, dm=False, v=False, xp=False,
-                    maxit=100000):
+                    maxit=100000, ru=None, matmul=None):
     """Multi-shift CG for (L + sigma + tau_j) U = W, W[:, c] = e_a - e_b for pairs[c].
+    matmul: callable x -> A @ x (default SciPy's product; a threaded one for large graphs).
 
     Returns (iterations of the seed system, G per column)."""
     n = A.shape[0]
@@ -48,6 +52,8 @@ def shortlist_solve(A, deg, sigma, tau, om, pairs, tol=1e-7, M=16, r=False, d=Fa
     p = len(tau)
     ident = lambda x: x
     rR, rD, rDm, rV, rX = (_f32 if k else ident for k in (r, d, dm, v, xp))
+    mul = matmul if matmul is not None else (lambda x: A @ x)
+    xs = np.zeros((n, R)) if ru else None
     res = W.copy()
     dirn = W.copy()
     rr = (res * res).sum(0)
@@ -69,10 +75,14 @@ def shortlist_solve(A, deg, sigma, tau, om, pairs, tol=1e-7, M=16, r=False, d=Fa
         if it >= maxit:
             raise RuntimeError("multi-shift CG iteration cap")
         dg = rDm(dirn)
-        vv = rV(diag[:, None] * dg + A @ dg)
+        vv = rV(diag[:, None] * dg + mul(dg))
         dv = (dg * vv).sum(0)
         a = np.where(act, rr / np.where(act, dv, 1.0), 0.0)
         rn = rR(res - a * vv)
+        if ru:
+            xs += a * dg
+            if (it + 1) % ru == 0:  # reliable update: the true residual, accumulated in FP64
+                rn = rR(np.where(act, W - (diag[:, None] * xs + mul(xs)), rn))
         rrn = (rn * rn).sum(0)
         be = np.where(act, rrn / np.where(act, rr, 1.0), 0.0)
         c = np.where(act, a * bp / ap, 0.0)

@@ -27,6 +27,8 @@ SCHEMES = {
     "r64": dict(d=True, dm=True, v=True, xp=True),
     "device": dict(dm=True, v=True, xp=True),
     "device_r32": dict(r=True, dm=True, v=True, xp=True),
+    "device_r32_ru50": dict(r=True, dm=True, v=True, xp=True, ru=50),
+    "all32_ru50": dict(r=True, d=True, dm=True, v=True, xp=True, ru=50),
 }
 
 
